@@ -1,0 +1,322 @@
+"""Benchmark of the B200 shallow-water step (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--arith exact|fast] [--rows 2048 --cols 2048]
+
+Workload: the 2048x2048 plain-forward-at-scale case -- synthetic urban DEM
+at dx = 1 m (plane of slope 0.003, 30 % seeded building blocks raised 10 m,
+streets 0.2 m lower), Manning n 0.015 on streets / 0.05 on blocks, a
+181-value Gamma hyetograph over 10,800 s, open east edge, CFL 0.9, dry
+threshold 1e-3 m.  The state starts ponded (5 cm on streets) and is spun up
+for 200 steps before warm-up, so the timed steps see moving water.
+
+A "step" is one finite-volume time step over the whole grid: CFL dt from the
+previous state's reduction, fluxes, update, friction, masks, and the next CFL
+reduction plus FP64 ledger, all inside the fused kernel.  ``value`` is
+cell-updates/s over K timed steps (CUDA events on the launching stream; the
+per-step working set is 134 MB -- five input planes and three output planes of
+16.8 MB -- above the 126 MB L2, so no flush is inserted).  ``e2e`` times
+``B200ShallowWaterSolver.run`` called with HOST NumPy state: host->device copy of
+the state, the adaptive run over the same simulated window, and the
+device->host copy of the final state.
+
+Multi-GPU: one process per GPU, each advancing its own replica of the domain
+(the single domain does not shard without a halo exchange, which this step
+does not implement); ``value`` is the sum over ranks divided by the slowest
+rank's time ("replicas", weak scaling).
+
+``--impl reference`` times the CPU implementation of the same path: the C
+restatement of the reference step (oracle/swe_oracle.c, OpenMP over all host
+threads) on the same workload, a few whole-grid steps per timed step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "gpu-hybrid-flood-forecasting_b200"))
+sys.path.insert(0, str(REPO))
+
+METRIC = "cell-updates/s (plain single-domain step, 2048x2048 urban)"
+BYTES_PER_CELL = 32  # h, hu, hv, bed, n^2 read (20 B) + h, hu, hv written (12 B)
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--arith", choices=["exact", "fast"], default="exact")
+    ap.add_argument("--rows", type=int, default=2048)
+    ap.add_argument("--cols", type=int, default=2048)
+    ap.add_argument("--spinup", type=int, default=200)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _workload(rows, cols):
+    from hybrid_flood_b200.workloads import urban
+
+    w = urban(rows, cols)
+    plane = 0.003 * (cols * 1.0 - (np.arange(cols) + 0.5))[None, :]
+    streets = (w.bed - plane) < 1.0
+    depth = np.where(streets, 0.05, 0.0).astype(np.float32)
+    return w, depth
+
+
+def _peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle-reason sampler running during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self._t:
+                self._t.join(timeout=2)
+
+    def summary(self) -> dict:
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def _cpu_port_time(w, depth, steps: int, threads: int):
+    """Time the C restatement of the reference step on the host: (s/step, cells)."""
+    from oracle import cport
+    from oracle import swe_numpy as O
+
+    p = O.make_params(w.bed, w.manning_n, w.domain_mask, **w.solver_kwargs())
+    d = cport.Domain(p)
+    cport.set_threads(threads)
+    st = O.initial_state(p, depth_m=depth)
+    t = 0.0
+    dt = d.cfl_dt(st)
+    st = d.step(st, dt, t)  # warm-up (first touch of the buffers)
+    t += dt
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = d.cfl_dt(st)
+        st = d.step(st, dt, t)
+        t += dt
+    el = time.perf_counter() - t0
+    return el / steps, w.bed.size
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    from oracle import cport
+
+    w, depth = _workload(args.rows, args.cols)
+    threads = cport.default_threads()
+    per_step, cells = _cpu_port_time(w, depth, max(1, args.steps // 40) + 1, threads)
+    # "steps" of this arm: K whole-grid steps, each timed as measured above.
+    k = args.steps
+    value = cells / per_step
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": k, "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"urban {args.rows}x{args.cols} dx=1m (plain forward at scale)",
+                   "cells": cells, "arith": "C restatement, IEEE float32, no FMA"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{max(1, args.steps // 40) + 1} whole-grid steps of the same workload"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, rank: int, world: int):
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        dist.init_process_group("nccl", device_id=dev)
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver, ledger_error
+
+    w, depth = _workload(args.rows, args.cols)
+    solver = B200ShallowWaterSolver(w.bed, w.manning_n, w.domain_mask, **w.solver_kwargs(),
+                                    arithmetic=args.arith, device=dev)
+    state = solver.initial_state(depth_m=depth)
+    t_sim, _, _ = solver.advance_(state, args.spinup, 0.0)
+    t_sim, _, _ = solver.advance_(state, args.warmup, t_sim)
+    cells = w.bed.size
+    stream = torch.cuda.current_stream(dev)
+    solver.set_timing(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_before = t_sim
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        t_sim, steps_used, ledger = solver.advance_(state, args.steps, t_sim)
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    kernel_ms, kernel_launches = solver.last_step_time()
+    launches = solver.last_launch_count()
+    if dist:
+        tt = torch.tensor([ms, kernel_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, kernel_ms = float(tt[0]), float(tt[1])
+    value = cells * args.steps * world / (ms / 1e3)
+    window = t_sim - t_before
+
+    # End to end through the public API with host buffers.
+    e2e = None
+    if not args.no_e2e:
+        host = [t.cpu().numpy().copy() for t in state]
+        pinned = [torch.from_numpy(a).pin_memory() for a in host]
+        times = np.asarray([0.0, window], np.float32)
+        r = solver.run(pinned, times)  # warm-up of the run path
+        torch.cuda.synchronize(dev)
+        reps = 3
+        t0 = time.perf_counter()
+        e_start = torch.cuda.Event(enable_timing=True)
+        e_end = torch.cuda.Event(enable_timing=True)
+        e_start.record(stream)
+        steps_e2e = 0
+        for _ in range(reps):
+            r = solver.run(pinned, times)
+            out = r.states.h[-1].cpu(), r.states.hu[-1].cpu(), r.states.hv[-1].cpu()
+            steps_e2e += r.steps_used
+        e_end.record(stream)
+        torch.cuda.synchronize(dev)
+        e_ms = e_start.elapsed_time(e_end)
+        wall = time.perf_counter() - t0
+        del out
+        plane = cells * 4
+        e2e = {"value": cells * steps_e2e * world / (e_ms / 1e3), "unit": "cell-updates/s",
+               "h2d_bytes_per_step": int(3 * plane * reps / max(steps_e2e, 1)),
+               "d2h_bytes_per_step": int(3 * plane * reps / max(steps_e2e, 1)),
+               "call": "B200ShallowWaterSolver.run(host NumPy state, [0, window]) + final state to host",
+               "steps_per_call": steps_e2e / reps, "wall_s": wall}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = _peaks()
+    per_launch_ms = kernel_ms / max(kernel_launches, 1)
+    achieved = BYTES_PER_CELL * cells / (per_launch_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"urban {args.rows}x{args.cols} dx=1m (plain forward at scale)",
+                   "cells_per_gpu": cells, "arith": args.arith, "parallelism": f"replicas{world}",
+                   "l2": "per-step working set 134 MB > 126 MB L2; no flush",
+                   "simulated_window_s": window, "spinup_steps": args.spinup},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "step_kernel (fused step + CFL + ledger)",
+                     "bytes_per_cell": BYTES_PER_CELL, "peak_kind": peak_kind,
+                     "kernel_ms_per_launch": per_launch_ms},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "ledger_rel_error": ledger_error(ledger),
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if not args.no_cpu_baseline:
+        from oracle import cport
+
+        threads = cport.default_threads()
+        per_step, _ = _cpu_port_time(w, depth, 3, threads)
+        line["cpu_baseline"] = {"value": cells / per_step, "unit": "cell-updates/s",
+                                "cores": threads, "kind": "port",
+                                "sample": "3 whole-grid steps of the same workload (C restatement)"}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = _args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.steps < 1 or args.warmup < 0:
+        raise SystemExit("--steps must be >= 1 and --warmup >= 0")
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_b200(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,642 @@
+// C-ABI of the B200 shallow-water step (declared in include/swe_b200.h).
+//
+// Host side: argument validation with the reference's error conventions,
+// packing of the static fields, launch planning, and the run driver.  The run
+// driver keeps the float64 clock, dt, output bookkeeping and mass ledger on
+// the device (swe::Control); the host enqueues step kernels in chunks and only
+// polls a pinned copy of the control block to learn when the run is done.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "swe_b200.h"
+#include "swe_step.cuh"
+
+using namespace swe;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define SWE_CK(expr)                                                                        \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(SWE_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int kThreads = 128;
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// Host restatement of np.interp for the plain-step entry point (float64, the
+// same expression order as the device version).
+double host_rain_rate(const std::vector<double>& t, const std::vector<double>& r, double dflt,
+                      double x) {
+    const int n = (int)t.size();
+    if (n <= 0) return dflt;
+    if (x != x) return x;
+    if (x < t[0] || x > t[n - 1]) return dflt;
+    if (n == 1 || x == t[n - 1]) return r[n - 1];
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (t[mid] <= x) lo = mid; else hi = mid;
+    }
+    if (x == t[lo]) return r[lo];
+    const volatile double slope = (r[lo + 1] - r[lo]) / (t[lo + 1] - t[lo]);
+    const volatile double prod = slope * (x - t[lo]);
+    double v = prod + r[lo];
+    if (v != v) {
+        const volatile double prod2 = slope * (x - t[lo + 1]);
+        v = prod2 + r[lo + 1];
+        if (v != v && r[lo] == r[lo + 1]) v = r[lo];
+    }
+    return v;
+}
+
+struct Plan {
+    int V;
+    int nstrips;
+    int rows_per_warp;
+    int blocks;
+};
+
+}  // namespace
+
+struct swe_domain {
+    DomainDev dd{};
+    int arith = SWE_ARITH_EXACT;
+    int device = 0;
+    int sms = 148;
+    float* bed = nullptr;
+    float* nm = nullptr;
+    float* mult = nullptr;
+    double* rain = nullptr;
+    std::vector<double> rain_t, rain_r;
+    Control* ctl = nullptr;          // run control (device)
+    Control* ctl_scratch = nullptr;  // standalone reductions (device)
+    Control* ctl_host = nullptr;     // pinned poll slots [2]
+    Partial* parts = nullptr;
+    int parts_cap = 0;
+    float* ping[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    int64_t ppitch = 0;
+    float* times_dev = nullptr;
+    int times_cap = 0;
+    cudaEvent_t poll_ev[2] = {nullptr, nullptr};
+    cudaEvent_t time_ev[2] = {nullptr, nullptr};
+    bool timing = false;
+    bool timed_valid = false;
+    int64_t timed_steps = 0;
+    int64_t launches = 0;
+    int rows_per_warp_override = 0;
+};
+
+namespace {
+
+Plan make_plan(const swe_domain* d, int V) {
+    Plan p;
+    p.V = V;
+    const int rows = d->dd.rows, cols = d->dd.cols;
+    p.nstrips = (cols + kWarp * V - 1) / (kWarp * V);
+    int R = d->rows_per_warp_override;
+    if (R <= 0) {
+        // Aim for ~32 resident warps per SM worth of work items, chunks of >= 8 rows.
+        const int64_t target = (int64_t)d->sms * 32;
+        R = (int)((int64_t)rows * p.nstrips / std::max<int64_t>(target, 1));
+        R = std::max(8, std::min(R, 64));
+    }
+    p.rows_per_warp = R;
+    const int64_t chunks = (rows + R - 1) / R;
+    const int64_t warps = chunks * p.nstrips;
+    const int wpb = kThreads / kWarp;
+    p.blocks = (int)((warps + wpb - 1) / wpb);
+    return p;
+}
+
+template <int V, class M, bool RUN>
+void launch_step_t(const Plan& pl, const StepLaunch& sl, cudaStream_t st) {
+    step_kernel<V, M, kThreads, RUN><<<pl.blocks, kThreads, 0, st>>>(sl);
+}
+
+template <class M, bool RUN>
+void launch_step_m(const Plan& pl, const StepLaunch& sl, cudaStream_t st) {
+    switch (pl.V) {
+        case 4: launch_step_t<4, M, RUN>(pl, sl, st); break;
+        case 2: launch_step_t<2, M, RUN>(pl, sl, st); break;
+        default: launch_step_t<1, M, RUN>(pl, sl, st); break;
+    }
+}
+
+void launch_step(const swe_domain* d, const Plan& pl, const StepLaunch& sl, bool run,
+                 cudaStream_t st) {
+    if (d->arith == SWE_ARITH_FAST) {
+        if (run) launch_step_m<FastMath, true>(pl, sl, st); else launch_step_m<FastMath, false>(pl, sl, st);
+    } else {
+        if (run) launch_step_m<ExactMath, true>(pl, sl, st); else launch_step_m<ExactMath, false>(pl, sl, st);
+    }
+}
+
+int reduce_blocks(const swe_domain* d) {
+    const int64_t n = (int64_t)d->dd.rows * d->dd.cols;
+    const int64_t want = (n + kThreads * 8 - 1) / (kThreads * 8);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)d->sms * 8));
+}
+
+void launch_reduce(const swe_domain* d, const StateView& s, Control* ctl, cudaStream_t st) {
+    const int blocks = reduce_blocks(d);
+    if (d->arith == SWE_ARITH_FAST)
+        reduce_kernel<FastMath, kThreads><<<blocks, kThreads, 0, st>>>(d->dd, s, ctl, d->parts);
+    else
+        reduce_kernel<ExactMath, kThreads><<<blocks, kThreads, 0, st>>>(d->dd, s, ctl, d->parts);
+}
+
+int choose_vec(const void* const* ptrs, int n, int64_t pitch_a, int64_t pitch_b) {
+    auto aligned = [&](int bytes) {
+        for (int i = 0; i < n; ++i)
+            if (reinterpret_cast<uintptr_t>(ptrs[i]) % bytes) return false;
+        return true;
+    };
+    if (pitch_a % 4 == 0 && pitch_b % 4 == 0 && aligned(16)) return 4;
+    if (pitch_a % 2 == 0 && pitch_b % 2 == 0 && aligned(8)) return 2;
+    return 1;
+}
+
+int ensure_parts(swe_domain* d, int blocks) {
+    if (blocks <= d->parts_cap) return SWE_OK;
+    if (d->parts) cudaFree(d->parts);
+    d->parts = nullptr;
+    SWE_CK(cudaMalloc(&d->parts, sizeof(Partial) * (size_t)blocks));
+    d->parts_cap = blocks;
+    return SWE_OK;
+}
+
+int ensure_ping(swe_domain* d) {
+    if (d->ping[0][0]) return SWE_OK;
+    d->ppitch = round_up(d->dd.cols, 32);
+    const size_t plane = sizeof(float) * (size_t)d->ppitch * (size_t)d->dd.rows;
+    for (int b = 0; b < 2; ++b)
+        for (int f = 0; f < 3; ++f) {
+            SWE_CK(cudaMalloc(&d->ping[b][f], plane));
+            SWE_CK(cudaMemset(d->ping[b][f], 0, plane));
+        }
+    return SWE_OK;
+}
+
+int check_state_ptrs(const void* a, const void* b, const void* c, int64_t pitch, int cols) {
+    if (!a || !b || !c) return fail(SWE_ERR_INVALID, "state pointers must be non-null");
+    if (pitch < cols) return fail(SWE_ERR_INVALID, "pitch must be >= cols");
+    return SWE_OK;
+}
+
+int copy_plane(float* dst, int64_t dpitch, const float* src, int64_t spitch, int rows, int cols,
+               cudaStream_t st) {
+    SWE_CK(cudaMemcpy2DAsync(dst, sizeof(float) * dpitch, src, sizeof(float) * spitch,
+                             sizeof(float) * cols, rows, cudaMemcpyDeviceToDevice, st));
+    return SWE_OK;
+}
+
+// Shared run driver for swe_run and swe_advance.
+int run_driver(swe_domain* d, StateView init, const float* times_host, int n_times,
+               double t_start, int n_out, int max_steps, float* out_h, float* out_hu,
+               float* out_hv, swe_run_result* res, cudaStream_t st, int* final_buf) {
+    const int rows = d->dd.rows, cols = d->dd.cols;
+    int rc = ensure_ping(d);
+    if (rc) return rc;
+    const Plan pl = make_plan(d, 2);
+    rc = ensure_parts(d, std::max(pl.blocks, reduce_blocks(d)));
+    if (rc) return rc;
+    for (int f = 0; f < 3; ++f) {
+        const float* src = f == 0 ? init.h : (f == 1 ? init.hu : init.hv);
+        rc = copy_plane(d->ping[0][f], d->ppitch, src, init.pitch, rows, cols, st);
+        if (rc) return rc;
+    }
+    if (n_times > d->times_cap) {
+        if (d->times_dev) cudaFree(d->times_dev);
+        d->times_dev = nullptr;
+        SWE_CK(cudaMalloc(&d->times_dev, sizeof(float) * (size_t)n_times));
+        d->times_cap = n_times;
+    }
+    SWE_CK(cudaMemcpyAsync(d->times_dev, times_host, sizeof(float) * (size_t)n_times,
+                           cudaMemcpyHostToDevice, st));
+    if (out_h) {
+        float* outs[3] = {out_h, out_hu, out_hv};
+        for (int f = 0; f < 3; ++f) {
+            const float* src = f == 0 ? init.h : (f == 1 ? init.hu : init.hv);
+            rc = copy_plane(outs[f], cols, src, init.pitch, rows, cols, st);
+            if (rc) return rc;
+        }
+    }
+    Control c0;
+    std::memset(&c0, 0, sizeof(c0));
+    c0.n_out = n_out;
+    c0.max_steps = max_steps;
+    c0.t_start = t_start;
+    c0.times = d->times_dev;
+    c0.out_h = out_h;
+    c0.out_hu = out_hu;
+    c0.out_hv = out_hv;
+    c0.out_plane = (int64_t)rows * cols;
+    c0.snap = -1;
+    // Pageable source: the copy is staged before cudaMemcpyAsync returns.
+    SWE_CK(cudaMemcpyAsync(d->ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, st));
+    StateView v0{d->ping[0][0], d->ping[0][1], d->ping[0][2], d->ppitch};
+    launch_reduce(d, v0, d->ctl, st);
+    SWE_CK(cudaGetLastError());
+    int64_t launched = 0;
+    d->launches = 1;
+    d->timed_valid = false;
+    if (d->timing) SWE_CK(cudaEventRecord(d->time_ev[0], st));
+    StepLaunch sl{};
+    sl.d = d->dd;
+    sl.ctl = d->ctl;
+    sl.parts = d->parts;
+    sl.nstrips = pl.nstrips;
+    sl.rows_per_warp = pl.rows_per_warp;
+    const int K = 32;
+    int chunk = 0;
+    bool finished = false;
+    while (!finished) {
+        const int64_t todo = std::min<int64_t>(K, (int64_t)max_steps - launched);
+        for (int64_t k = 0; k < todo; ++k) {
+            const int src = (int)((launched + k) & 1);
+            sl.in = StateView{d->ping[src][0], d->ping[src][1], d->ping[src][2], d->ppitch};
+            sl.out = StateOut{d->ping[src ^ 1][0], d->ping[src ^ 1][1], d->ping[src ^ 1][2], d->ppitch};
+            launch_step(d, pl, sl, true, st);
+        }
+        SWE_CK(cudaGetLastError());
+        launched += todo;
+        d->launches += todo;
+        const int slot = chunk & 1;
+        SWE_CK(cudaMemcpyAsync(&d->ctl_host[slot], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+        SWE_CK(cudaEventRecord(d->poll_ev[slot], st));
+        if (launched >= max_steps) break;
+        if (chunk > 0) {
+            SWE_CK(cudaEventSynchronize(d->poll_ev[slot ^ 1]));
+            if (d->ctl_host[slot ^ 1].done) finished = true;
+        }
+        ++chunk;
+    }
+    if (d->timing) {
+        // The end event follows the last step kernel; poll copies in between are ~1 us each.
+        SWE_CK(cudaEventRecord(d->time_ev[1], st));
+        d->timed_steps = launched;
+        d->timed_valid = true;
+    }
+    SWE_CK(cudaStreamSynchronize(st));
+    SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
+    const Control& c = d->ctl_host[0];
+    res->final_time_s = c.t;
+    res->outputs_written = c.idx;
+    res->steps_used = c.steps;
+    res->status = c.status ? c.status : (c.idx >= n_out ? SWE_OK : SWE_ERR_MAX_STEPS);
+    res->reserved = 0;
+    for (int i = 0; i < 6; ++i) res->ledger[i] = c.ledger[i];
+    if (final_buf) *final_buf = c.steps & 1;
+    return SWE_OK;
+}
+
+void free_domain(swe_domain* d) {
+    if (!d) return;
+    cudaFree(d->bed);
+    cudaFree(d->nm);
+    cudaFree(d->mult);
+    cudaFree(d->rain);
+    cudaFree(d->ctl);
+    cudaFree(d->ctl_scratch);
+    if (d->ctl_host) cudaFreeHost(d->ctl_host);
+    cudaFree(d->parts);
+    for (int b = 0; b < 2; ++b)
+        for (int f = 0; f < 3; ++f) cudaFree(d->ping[b][f]);
+    cudaFree(d->times_dev);
+    for (int i = 0; i < 2; ++i) {
+        if (d->poll_ev[i]) cudaEventDestroy(d->poll_ev[i]);
+        if (d->time_ev[i]) cudaEventDestroy(d->time_ev[i]);
+    }
+    delete d;
+}
+
+__global__ void pack_static_kernel(const float* bed, const float* man, const uint8_t* mask,
+                                   const float* mult, int rows, int cols, int64_t pitch,
+                                   float* bed_o, float* nm_o, float* mult_o) {
+    const int64_t n = (int64_t)rows * pitch;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / pitch), c = (int)(i - (int64_t)r * pitch);
+        const int cc = c < cols ? c : cols - 1;
+        const int64_t j = (int64_t)r * cols + cc;
+        const float n_ = man[j];
+        const float n2 = __fmul_rn(n_, n_);  // manning_n**2 in float32
+        const float n2a = fabsf(n2);
+        bed_o[i] = bed[j];
+        // The domain mask rides in the sign bit: set = inactive.
+        nm_o[i] = mask[j] ? n2a : __int_as_float(__float_as_int(n2a) | (int)0x80000000);
+        if (mult_o) mult_o[i] = mult[j];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* swe_version(void) { return "swe_b200 0.1.0 sm_100a"; }
+
+int swe_last_error(char* buf, size_t n) {
+    if (buf && n) {
+        const size_t k = std::min(n - 1, g_err.size());
+        std::memcpy(buf, g_err.data(), k);
+        buf[k] = '\0';
+    }
+    return (int)g_err.size();
+}
+
+int swe_domain_create(const swe_domain_desc* desc, swe_domain_t* out) {
+    if (!desc || !out) return fail(SWE_ERR_INVALID, "null descriptor or output handle");
+    *out = nullptr;
+    const swe_domain_desc& q = *desc;
+    if (q.rows < 1 || q.cols < 1) return fail(SWE_ERR_INVALID, "rows and cols must be >= 1");
+    if (!(q.dx > 0) || !(q.dy > 0)) return fail(SWE_ERR_INVALID, "dx and dy must be positive");
+    if (!(q.max_dt > 0)) return fail(SWE_ERR_INVALID, "max_dt must be positive");
+    if (!(q.dry_tolerance >= 0)) return fail(SWE_ERR_INVALID, "dry_tolerance must be >= 0");
+    if (q.n_rain < 1 || !q.rain_times || !q.rain_rates)
+        return fail(SWE_ERR_INVALID, "the hyetograph needs at least one (time, rate) pair");
+    for (int i = 0; i < 4; ++i)
+        if (q.boundary[i] != SWE_REFLECTIVE && q.boundary[i] != SWE_OPEN)
+            return fail(SWE_ERR_INVALID, "boundary codes must be 0 (reflective) or 1 (open)");
+    if (!q.bed || !q.manning_n || !q.domain_mask)
+        return fail(SWE_ERR_INVALID, "bed, manning_n and domain_mask are required");
+    if (q.arithmetic != SWE_ARITH_EXACT && q.arithmetic != SWE_ARITH_FAST)
+        return fail(SWE_ERR_INVALID, "arithmetic must be SWE_ARITH_EXACT or SWE_ARITH_FAST");
+    int dev = 0;
+    SWE_CK(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    SWE_CK(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10)
+        return fail(SWE_ERR_NO_DEVICE, std::string("this build targets sm_100a; device is ") + prop.name);
+
+    swe_domain* d = new swe_domain();
+    d->device = dev;
+    d->sms = prop.multiProcessorCount;
+    d->arith = q.arithmetic;
+    if (const char* e = std::getenv("SWE_ROWS_PER_WARP")) d->rows_per_warp_override = std::atoi(e);
+    const int rows = q.rows, cols = q.cols;
+    const int64_t pitch = round_up(cols, 32);
+    const size_t plane = sizeof(float) * (size_t)pitch * rows;
+    const size_t n = (size_t)rows * cols;
+    auto bail = [&](int code) { free_domain(d); return code; };
+    cudaError_t e;
+#define SWE_CK2(expr)                                                                          \
+    do {                                                                                       \
+        e = (expr);                                                                            \
+        if (e != cudaSuccess)                                                                  \
+            return bail(fail(SWE_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e))); \
+    } while (0)
+    SWE_CK2(cudaMalloc(&d->bed, plane));
+    SWE_CK2(cudaMalloc(&d->nm, plane));
+    if (q.rainfall_multiplier) SWE_CK2(cudaMalloc(&d->mult, plane));
+    // Stage the inputs on the device, then pack.
+    const float *bed_s = q.bed, *man_s = q.manning_n, *mult_s = q.rainfall_multiplier;
+    const uint8_t* mask_s = q.domain_mask;
+    void* staging = nullptr;
+    if (q.fields_on_host) {
+        const size_t bytes = n * (3 * sizeof(float) + 1) + 256;
+        SWE_CK2(cudaMalloc(&staging, bytes));
+        char* p = static_cast<char*>(staging);
+        SWE_CK2(cudaMemcpy(p, q.bed, n * sizeof(float), cudaMemcpyHostToDevice));
+        bed_s = reinterpret_cast<const float*>(p);
+        p += n * sizeof(float);
+        SWE_CK2(cudaMemcpy(p, q.manning_n, n * sizeof(float), cudaMemcpyHostToDevice));
+        man_s = reinterpret_cast<const float*>(p);
+        p += n * sizeof(float);
+        if (q.rainfall_multiplier) {
+            SWE_CK2(cudaMemcpy(p, q.rainfall_multiplier, n * sizeof(float), cudaMemcpyHostToDevice));
+            mult_s = reinterpret_cast<const float*>(p);
+        }
+        p += n * sizeof(float);
+        SWE_CK2(cudaMemcpy(p, q.domain_mask, n, cudaMemcpyHostToDevice));
+        mask_s = reinterpret_cast<const uint8_t*>(p);
+    }
+    pack_static_kernel<<<std::min<int64_t>((rows * pitch + 255) / 256, 4096), 256>>>(
+        bed_s, man_s, mask_s, mult_s, rows, cols, pitch, d->bed, d->nm, d->mult);
+    SWE_CK2(cudaGetLastError());
+    SWE_CK2(cudaDeviceSynchronize());
+    if (staging) cudaFree(staging);
+    // Hyetograph as float64 (np.interp converts the float32 table to float64).
+    d->rain_t.resize(q.n_rain);
+    d->rain_r.resize(q.n_rain);
+    for (int i = 0; i < q.n_rain; ++i) {
+        d->rain_t[i] = (double)q.rain_times[i];
+        d->rain_r[i] = (double)q.rain_rates[i];
+    }
+    SWE_CK2(cudaMalloc(&d->rain, sizeof(double) * 2 * q.n_rain));
+    SWE_CK2(cudaMemcpy(d->rain, d->rain_t.data(), sizeof(double) * q.n_rain, cudaMemcpyHostToDevice));
+    SWE_CK2(cudaMemcpy(d->rain + q.n_rain, d->rain_r.data(), sizeof(double) * q.n_rain,
+                       cudaMemcpyHostToDevice));
+    SWE_CK2(cudaMalloc(&d->ctl, sizeof(Control)));
+    SWE_CK2(cudaMalloc(&d->ctl_scratch, sizeof(Control)));
+    SWE_CK2(cudaMemset(d->ctl, 0, sizeof(Control)));
+    SWE_CK2(cudaMemset(d->ctl_scratch, 0, sizeof(Control)));
+    SWE_CK2(cudaMallocHost(&d->ctl_host, 2 * sizeof(Control)));
+    for (int i = 0; i < 2; ++i) SWE_CK2(cudaEventCreateWithFlags(&d->poll_ev[i], cudaEventDisableTiming));
+#undef SWE_CK2
+
+    DomainDev& dd = d->dd;
+    dd.rows = rows;
+    dd.cols = cols;
+    dd.spitch = pitch;
+    dd.bed = d->bed;
+    dd.nm = d->nm;
+    dd.mult = d->mult;
+    for (int i = 0; i < 4; ++i) dd.bnd[i] = q.boundary[i];
+    dd.k.g = (float)q.gravity;
+    dd.k.half_g = (float)(0.5 * q.gravity);
+    dd.k.dry = (float)q.dry_tolerance;
+    dd.k.dx = (float)q.dx;
+    dd.k.dy = (float)q.dy;
+    dd.k.eps = (float)1.0e-12;
+    dd.k.expo = (float)(7.0 / 3.0);
+    dd.dx = q.dx;
+    dd.dy = q.dy;
+    dd.g = q.gravity;
+    dd.cfl = q.cfl;
+    dd.max_dt = q.max_dt;
+    dd.default_rain = q.default_rainfall;
+    dd.rain_t = d->rain;
+    dd.rain_r = d->rain + q.n_rain;
+    dd.n_rain = q.n_rain;
+    *out = d;
+    return SWE_OK;
+}
+
+int swe_domain_destroy(swe_domain_t d) {
+    if (!d) return SWE_OK;
+    cudaDeviceSynchronize();
+    free_domain(d);
+    return SWE_OK;
+}
+
+int swe_rainfall_rate(swe_domain_t d, double time_s, double* rate_out) {
+    if (!d || !rate_out) return fail(SWE_ERR_INVALID, "null argument");
+    *rate_out = host_rain_rate(d->rain_t, d->rain_r, d->dd.default_rain, time_s);
+    return SWE_OK;
+}
+
+int swe_step(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch_in,
+             float* h_out, float* hu_out, float* hv_out, int64_t pitch_out, double dt,
+             double time_s, void* stream) {
+    if (!d) return fail(SWE_ERR_INVALID, "null domain");
+    int rc = check_state_ptrs(h, hu, hv, pitch_in, d->dd.cols);
+    if (rc) return rc;
+    rc = check_state_ptrs(h_out, hu_out, hv_out, pitch_out, d->dd.cols);
+    if (rc) return rc;
+    const void* ins[3] = {h, hu, hv};
+    const void* outs[3] = {h_out, hu_out, hv_out};
+    for (auto a : ins)
+        for (auto b : outs)
+            if (a == b) return fail(SWE_ERR_INVALID, "step outputs must not alias its inputs");
+    const void* all[6] = {h, hu, hv, h_out, hu_out, hv_out};
+    const int V = choose_vec(all, 6, pitch_in, pitch_out);
+    const Plan pl = make_plan(d, V);
+    const double rate = host_rain_rate(d->rain_t, d->rain_r, d->dd.default_rain, time_s);
+    StepLaunch sl{};
+    sl.d = d->dd;
+    sl.in = StateView{h, hu, hv, pitch_in};
+    sl.out = StateOut{h_out, hu_out, hv_out, pitch_out};
+    sl.s.dt = (float)dt;
+    const volatile double dr = dt * rate;
+    const volatile double dg = dt * d->dd.g;
+    sl.s.dt_rain = (float)dr;
+    sl.s.dt_g = (float)dg;
+    sl.ctl = nullptr;
+    sl.parts = nullptr;
+    sl.nstrips = pl.nstrips;
+    sl.rows_per_warp = pl.rows_per_warp;
+    launch_step(d, pl, sl, false, static_cast<cudaStream_t>(stream));
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
+int swe_max_inverse_dt(swe_domain_t d, const float* h, const float* hu, const float* hv,
+                       int64_t pitch, float* max_inverse_dt_out, void* stream) {
+    if (!d || !max_inverse_dt_out) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    rc = ensure_parts(d, reduce_blocks(d));
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Control c0;
+    std::memset(&c0, 0, sizeof(c0));
+    c0.snap = -1;
+    SWE_CK(cudaMemcpyAsync(d->ctl_scratch, &c0, sizeof(Control), cudaMemcpyHostToDevice, st));
+    launch_reduce(d, StateView{h, hu, hv, pitch}, d->ctl_scratch, st);
+    SWE_CK(cudaGetLastError());
+    SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl_scratch, sizeof(Control), cudaMemcpyDeviceToHost, st));
+    SWE_CK(cudaStreamSynchronize(st));
+    *max_inverse_dt_out = d->ctl_host[0].maxinv;
+    return SWE_OK;
+}
+
+int swe_cfl_dt(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch,
+               double* dt_out, void* stream) {
+    if (!dt_out) return fail(SWE_ERR_INVALID, "null argument");
+    float m = 0.f;
+    const int rc = swe_max_inverse_dt(d, h, hu, hv, pitch, &m, stream);
+    if (rc) return rc;
+    const double md = (double)m;
+    if (md > 0.0) {
+        const double c = d->dd.cfl / md;
+        *dt_out = c < d->dd.max_dt ? c : d->dd.max_dt;
+    } else {
+        *dt_out = d->dd.max_dt;
+    }
+    return SWE_OK;
+}
+
+int swe_run(swe_domain_t d, const float* h0, const float* hu0, const float* hv0, int64_t pitch_in,
+            const float* output_times, int32_t n_out, int32_t max_steps, float* out_h,
+            float* out_hu, float* out_hv, swe_run_result* result, void* stream) {
+    if (!d || !result) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h0, hu0, hv0, pitch_in, d->dd.cols);
+    if (rc) return rc;
+    if (!output_times || n_out < 1)
+        return fail(SWE_ERR_INVALID, "Output times must be one-dimensional, start at zero, and increase.");
+    if (output_times[0] != 0.0f)
+        return fail(SWE_ERR_INVALID, "Output times must be one-dimensional, start at zero, and increase.");
+    for (int i = 1; i < n_out; ++i)
+        if (!(output_times[i] > output_times[i - 1]))
+            return fail(SWE_ERR_INVALID, "Output times must be one-dimensional, start at zero, and increase.");
+    if (max_steps < 0) return fail(SWE_ERR_INVALID, "max_steps must be >= 0");
+    if (!out_h || !out_hu || !out_hv) return fail(SWE_ERR_INVALID, "output buffers are required");
+    rc = run_driver(d, StateView{h0, hu0, hv0, pitch_in}, output_times, n_out,
+                    (double)output_times[0], n_out, max_steps, out_h, out_hu, out_hv, result,
+                    static_cast<cudaStream_t>(stream), nullptr);
+    if (rc) return rc;
+    if (result->status == SWE_ERR_MAX_STEPS) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "max_steps=%d wrote %d/%d outputs; last time=%.3f s.",
+                      max_steps, result->outputs_written, n_out, result->final_time_s);
+        return fail(SWE_ERR_MAX_STEPS, msg);
+    }
+    if (result->status == SWE_ERR_NONFINITE)
+        return fail(SWE_ERR_NONFINITE, "non-finite values reached the CFL reduction");
+    return SWE_OK;
+}
+
+int swe_advance(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, int32_t n_steps,
+                double start_s, swe_run_result* result, void* stream) {
+    if (!d || !result) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    if (n_steps < 0) return fail(SWE_ERR_INVALID, "n_steps must be >= 0");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float times[2] = {(float)start_s, INFINITY};
+    int fb = 0;
+    rc = run_driver(d, StateView{h, hu, hv, pitch}, times, 2, start_s, 2, n_steps, nullptr,
+                    nullptr, nullptr, result, st, &fb);
+    if (rc) return rc;
+    if (result->status == SWE_ERR_NONFINITE)
+        return fail(SWE_ERR_NONFINITE, "non-finite values reached the CFL reduction");
+    result->status = SWE_OK;
+    float* outs[3] = {h, hu, hv};
+    for (int f = 0; f < 3; ++f) {
+        rc = copy_plane(outs[f], pitch, d->ping[fb][f], d->ppitch, d->dd.rows, d->dd.cols, st);
+        if (rc) return rc;
+    }
+    SWE_CK(cudaStreamSynchronize(st));
+    return SWE_OK;
+}
+
+int64_t swe_last_launch_count(swe_domain_t d) { return d ? d->launches : -1; }
+
+int swe_set_timing(swe_domain_t d, int32_t enable) {
+    if (!d) return fail(SWE_ERR_INVALID, "null domain");
+    if (enable && !d->time_ev[0]) {
+        SWE_CK(cudaEventCreate(&d->time_ev[0]));
+        SWE_CK(cudaEventCreate(&d->time_ev[1]));
+    }
+    d->timing = enable != 0;
+    return SWE_OK;
+}
+
+int swe_last_step_time(swe_domain_t d, double* ms, int64_t* step_launches) {
+    if (!d || !ms || !step_launches) return fail(SWE_ERR_INVALID, "null argument");
+    if (!d->timed_valid) return fail(SWE_ERR_INVALID, "no timed run recorded (call swe_set_timing first)");
+    float f = 0.f;
+    SWE_CK(cudaEventElapsedTime(&f, d->time_ev[0], d->time_ev[1]));
+    *ms = (double)f;
+    *step_launches = d->timed_steps;
+    return SWE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,712 @@
+// Fused shallow-water step kernels for sm_100a.
+//
+// One step of the reference finite-volume scheme
+// (src/hybrid_flood/numpy_solver/shallow_water_2d.py:277-327, the same
+// arithmetic as src/hybrid_flood/jax_solver/numerics.py:312-369) in ONE kernel:
+// ghost ring, wall mirroring, hydrostatic reconstruction, HLL x/y fluxes,
+// divergence, rain source, positivity clip, semi-implicit Manning friction,
+// wet/dry masking -- and, in run mode, the CFL inverse-dt reduction of the NEW
+// state (numerics.py:297-309) plus FP64 mass-ledger partials, finished by the
+// last CTA, which also advances the device-resident FP64 clock.
+//
+// Work decomposition ("column marching"): a warp owns a strip of 32*V columns
+// (V consecutive columns per lane, loaded as float2/float4) and marches up a
+// chunk of rows.  Every x-face and y-face inside the strip is evaluated once:
+// the y-face above row r is carried in registers to row r+1, x-faces between
+// lanes travel by warp shuffle.  Only the chunk's bottom y-face row and the
+// strip's left x-face column are evaluated twice (once by each neighbour).
+// No shared memory and no block-wide barrier is needed inside the march.
+//
+// HBM traffic per cell-update: h, hu, hv, bed and n^2 (with the domain mask in
+// the sign bit of n^2) read once = 20 B, h, hu, hv written once = 12 B.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "swe_math.cuh"
+
+namespace swe {
+
+constexpr int kWarp = 32;
+
+// Float32 constants of the step, rounded from the float64 controls exactly where
+// NumPy's weak-scalar rule rounds them in the reference.
+struct Consts {
+    float g;       // float(g)
+    float half_g;  // float(0.5 * g)
+    float dry;     // float(dry_tolerance)
+    float dx, dy;  // float(dx), float(dy)
+    float eps;     // float(1e-12)   HLL denominator guard
+    float expo;    // float(7/3)     Manning exponent
+};
+
+// Per-step float32 scalars: float(dt), float(dt*rate), float(dt*g).
+struct StepScalars {
+    float dt, dt_rain, dt_g;
+};
+
+struct DomainDev {
+    int rows, cols;
+    int64_t spitch;      // pitch (elements) of the static planes
+    const float* bed;    // rows x spitch
+    const float* nm;     // n^2 with sign bit set on inactive cells
+    const float* mult;   // rain multiplier plane, or nullptr (= domain mask)
+    int bnd[4];          // left, right, bottom, top: 0 reflective, 1 open
+    Consts k;
+    double dx, dy, g, cfl, max_dt, default_rain;
+    const double* rain_t;  // hyetograph times (s), float64 copies of the float32 table
+    const double* rain_r;  // rates (m/s)
+    int n_rain;
+};
+
+struct StateView {
+    const float* h;
+    const float* hu;
+    const float* hv;
+    int64_t pitch;
+};
+
+struct StateOut {
+    float* h;
+    float* hu;
+    float* hv;
+    int64_t pitch;
+};
+
+// Device-resident run control: clock, next dt, output bookkeeping, ledger.
+struct Control {
+    double t;          // simulated time at the start of the next step
+    double dt;         // dt of the next step (already limited by the output target)
+    StepScalars s;     // float32 scalars of the next step
+    int snap;          // output index written by the next step, -1 if none
+    int idx;           // next output index to fill
+    int steps;         // steps taken
+    int done;          // nonzero: all outputs written, step cap hit or failure
+    int status;        // 0 ok, else an SWE_ERR_* code
+    float maxinv;      // max inverse CFL dt of the current state
+    unsigned counter;  // last-CTA ticket
+    int n_out, max_steps;
+    double t_start;               // clock value set by the init reduction
+    const float* times;           // device copy of the float32 output times
+    float* out_h;                 // n_out x rows x cols snapshots (may be null)
+    float* out_hu;
+    float* out_hv;
+    int64_t out_plane;            // rows * cols
+    double ledger[6];             // volume0, volume, rain_in, outflow, clip_gain, mask_loss
+};
+
+struct Partial {
+    float maxinv;
+    int bad;
+    double vol, rain, outflow, clip, mask;
+};
+
+// ---------------------------------------------------------------------------
+// Cells
+// ---------------------------------------------------------------------------
+struct Cell {
+    float h, hu, hv, z, nm;  // nm: n^2, negative (sign bit) = inactive
+    float u, v;              // cell velocities (unreconstructed depth)
+};
+
+__device__ __forceinline__ bool active(float nm) { return !signbit(nm); }
+
+template <class M>
+__device__ __forceinline__ void set_vel(Cell& c, float dry) {
+    M::vel2(c.hu, c.hv, c.h, dry, c.u, c.v);
+}
+
+// Load V cells of row r starting at column c0 (r in [-1, rows], c0 in [-V, cols]),
+// applying the ghost ring: clamp to the nearest interior cell, negate hu on
+// reflective left/right ghosts and hv on reflective bottom/top ghosts.
+template <int V>
+__device__ __forceinline__ void load_cells(const DomainDev& d, const StateView& s, int r, int c0,
+                                           Cell (&out)[V]) {
+    const int rr = r < 0 ? 0 : (r >= d.rows ? d.rows - 1 : r);
+    const bool flip_v = (r < 0 && d.bnd[2] == 0) || (r >= d.rows && d.bnd[3] == 0);
+    const int64_t so = (int64_t)rr * s.pitch;
+    const int64_t zo = (int64_t)rr * d.spitch;
+    if (c0 >= 0 && c0 + V <= d.cols) {
+        if constexpr (V == 4) {
+            const float4 h = __ldg(reinterpret_cast<const float4*>(s.h + so + c0));
+            const float4 hu = __ldg(reinterpret_cast<const float4*>(s.hu + so + c0));
+            const float4 hv = __ldg(reinterpret_cast<const float4*>(s.hv + so + c0));
+            const float4 z = __ldg(reinterpret_cast<const float4*>(d.bed + zo + c0));
+            const float4 nm = __ldg(reinterpret_cast<const float4*>(d.nm + zo + c0));
+            out[0] = {h.x, hu.x, hv.x, z.x, nm.x, 0.f, 0.f};
+            out[1] = {h.y, hu.y, hv.y, z.y, nm.y, 0.f, 0.f};
+            out[2] = {h.z, hu.z, hv.z, z.z, nm.z, 0.f, 0.f};
+            out[3] = {h.w, hu.w, hv.w, z.w, nm.w, 0.f, 0.f};
+        } else if constexpr (V == 2) {
+            const float2 h = __ldg(reinterpret_cast<const float2*>(s.h + so + c0));
+            const float2 hu = __ldg(reinterpret_cast<const float2*>(s.hu + so + c0));
+            const float2 hv = __ldg(reinterpret_cast<const float2*>(s.hv + so + c0));
+            const float2 z = __ldg(reinterpret_cast<const float2*>(d.bed + zo + c0));
+            const float2 nm = __ldg(reinterpret_cast<const float2*>(d.nm + zo + c0));
+            out[0] = {h.x, hu.x, hv.x, z.x, nm.x, 0.f, 0.f};
+            out[1] = {h.y, hu.y, hv.y, z.y, nm.y, 0.f, 0.f};
+        } else {
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+                out[i] = {__ldg(s.h + so + c0 + i), __ldg(s.hu + so + c0 + i),
+                          __ldg(s.hv + so + c0 + i), __ldg(d.bed + zo + c0 + i),
+                          __ldg(d.nm + zo + c0 + i), 0.f, 0.f};
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < V; ++i)
+            if (flip_v) out[i].hv = -out[i].hv;
+    } else {
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const int c = c0 + i;
+            const int cc = c < 0 ? 0 : (c >= d.cols ? d.cols - 1 : c);
+            Cell x = {__ldg(s.h + so + cc), __ldg(s.hu + so + cc), __ldg(s.hv + so + cc),
+                      __ldg(d.bed + zo + cc), __ldg(d.nm + zo + cc), 0.f, 0.f};
+            if ((c < 0 && d.bnd[0] == 0) || (c >= d.cols && d.bnd[1] == 0)) x.hu = -x.hu;
+            if (flip_v) x.hv = -x.hv;
+            out[i] = x;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Faces
+// ---------------------------------------------------------------------------
+// Flux through one face plus the two side-specific pressure corrections
+// (shallow_water_2d.py:138-239).  The lower-index cell sees F + corr_lo on the
+// normal-momentum component, the higher-index cell F + corr_hi.
+struct FaceFlux {
+    float f0, f1, f2;
+    float corr_lo, corr_hi;
+};
+
+// AXIS 1: x-face (normal momentum hu), AXIS 0: y-face (normal momentum hv).
+template <int AXIS, class M>
+__device__ __forceinline__ FaceFlux face_flux(const Cell& lo, const Cell& hi, const Consts& k) {
+    const bool a_lo = active(lo.nm), a_hi = active(hi.nm);
+    const bool relevant = a_lo | a_hi;
+    const bool hi_wall = a_lo & !a_hi;  // mirror lo onto hi
+    const bool lo_wall = !a_lo & a_hi;  // mirror hi onto lo
+    // Mirrored states: the normal-momentum velocity changes sign, the rest is copied.
+    const float hL = lo_wall ? hi.h : lo.h;
+    const float zL = lo_wall ? hi.z : lo.z;
+    const float hR = hi_wall ? lo.h : hi.h;
+    const float zR = hi_wall ? lo.z : hi.z;
+    float uL, vL, uR, vR;
+    if (AXIS == 1) {
+        uL = lo_wall ? -hi.u : lo.u;
+        vL = lo_wall ? hi.v : lo.v;
+        uR = hi_wall ? -lo.u : hi.u;
+        vR = hi_wall ? lo.v : hi.v;
+    } else {
+        uL = lo_wall ? hi.u : lo.u;
+        vL = lo_wall ? -hi.v : lo.v;
+        uR = hi_wall ? lo.u : hi.u;
+        vR = hi_wall ? -lo.v : hi.v;
+    }
+    // Hydrostatic reconstruction.
+    const float zf = fmaxf(zL, zR);
+    const float HL = fmaxf(M::sub(M::add(hL, zL), zf), 0.0f);
+    const float HR = fmaxf(M::sub(M::add(hR, zR), zf), 0.0f);
+    const float XL = M::mul(HL, uL), YL = M::mul(HL, vL);
+    const float XR = M::mul(HR, uR), YR = M::mul(HR, vR);
+    // HLL (shallow_water_2d.py:66-135) on the reconstructed states.
+    const float unL = AXIS == 1 ? M::recon_vel(XL, HL, k.dry, uL) : M::recon_vel(YL, HL, k.dry, vL);
+    const float unR = AXIS == 1 ? M::recon_vel(XR, HR, k.dry, uR) : M::recon_vel(YR, HR, k.dry, vR);
+    const float cL = M::sqrt(M::mul(k.g, HL));
+    const float cR = M::sqrt(M::mul(k.g, HR));
+    const float sL = fminf(M::sub(unL, cL), M::sub(unR, cR));
+    const float sR = fmaxf(M::add(unL, cL), M::add(unR, cR));
+    const float pL = M::mul(k.half_g, M::mul(HL, HL));
+    const float pR = M::mul(k.half_g, M::mul(HR, HR));
+    float fL0, fL1, fL2, fR0, fR1, fR2;
+    if (AXIS == 1) {
+        fL0 = XL;
+        fL1 = M::add(M::mul(XL, unL), pL);
+        fL2 = M::mul(XL, M::recon_vel(YL, HL, k.dry, vL));
+        fR0 = XR;
+        fR1 = M::add(M::mul(XR, unR), pR);
+        fR2 = M::mul(XR, M::recon_vel(YR, HR, k.dry, vR));
+    } else {
+        fL0 = YL;
+        fL1 = M::mul(XL, unL);
+        fL2 = M::add(M::mul(YL, unL), pL);
+        fR0 = YR;
+        fR1 = M::mul(XR, unR);
+        fR2 = M::add(M::mul(YR, unR), pR);
+    }
+    const float spread = M::sub(sR, sL);
+    const float den = spread > k.eps ? spread : 1.0f;
+    const float rden = M::recip(den);
+    const float s01 = M::mul(sL, sR);
+    const float m0 = M::over(M::add(M::sub(M::mul(sR, fL0), M::mul(sL, fR0)), M::mul(s01, M::sub(HR, HL))), rden);
+    const float m1 = M::over(M::add(M::sub(M::mul(sR, fL1), M::mul(sL, fR1)), M::mul(s01, M::sub(XR, XL))), rden);
+    const float m2 = M::over(M::add(M::sub(M::mul(sR, fL2), M::mul(sL, fR2)), M::mul(s01, M::sub(YR, YL))), rden);
+    const bool take_l = sL >= 0.0f, take_r = sR <= 0.0f;
+    FaceFlux f;
+    f.f0 = relevant ? (take_l ? fL0 : (take_r ? fR0 : m0)) : 0.0f;
+    f.f1 = relevant ? (take_l ? fL1 : (take_r ? fR1 : m1)) : 0.0f;
+    f.f2 = relevant ? (take_l ? fL2 : (take_r ? fR2 : m2)) : 0.0f;
+    f.corr_lo = relevant ? M::mul(k.half_g, M::sub(M::mul(hL, hL), M::mul(HL, HL))) : 0.0f;
+    f.corr_hi = relevant ? M::mul(k.half_g, M::sub(M::mul(hR, hR), M::mul(HR, HR))) : 0.0f;
+    return f;
+}
+
+// ---------------------------------------------------------------------------
+// Run-mode helpers
+// ---------------------------------------------------------------------------
+// np.interp(t, times, rates, left=default, right=default) in float64 with
+// separately rounded operations (shallow_water_2d.py:254-264).
+__device__ inline double rain_rate(const DomainDev& d, double t) {
+    const int n = d.n_rain;
+    if (n <= 0) return d.default_rain;
+    const double x0 = d.rain_t[0], xn = d.rain_t[n - 1];
+    if (t != t) return t;
+    if (t < x0 || t > xn) return d.default_rain;
+    if (n == 1 || t == xn) return d.rain_r[n - 1];
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (d.rain_t[mid] <= t) lo = mid; else hi = mid;
+    }
+    const double xj = d.rain_t[lo], yj = d.rain_r[lo];
+    if (t == xj) return yj;
+    const double xj1 = d.rain_t[lo + 1], yj1 = d.rain_r[lo + 1];
+    const double slope = __ddiv_rn(__dsub_rn(yj1, yj), __dsub_rn(xj1, xj));
+    double v = __dadd_rn(__dmul_rn(slope, __dsub_rn(t, xj)), yj);
+    if (v != v) {
+        v = __dadd_rn(__dmul_rn(slope, __dsub_rn(t, xj1)), yj1);
+        if (v != v && yj == yj1) v = yj;
+    }
+    return v;
+}
+
+// Float32 scalars of a step of length dt starting at t.
+__device__ inline StepScalars step_scalars(const DomainDev& d, double dt, double t) {
+    StepScalars s;
+    s.dt = __double2float_rn(dt);
+    s.dt_rain = __double2float_rn(__dmul_rn(dt, rain_rate(d, t)));
+    s.dt_g = __double2float_rn(__dmul_rn(dt, d.g));
+    return s;
+}
+
+// CFL dt from the largest inverse dt (shallow_water_2d.py:274; in float64).
+__device__ inline double cfl_dt_from(const DomainDev& d, float maxinv) {
+    const double m = (double)maxinv;
+    if (m > 0.0) {
+        const double c = __ddiv_rn(d.cfl, m);
+        return c < d.max_dt ? c : d.max_dt;
+    }
+    return d.max_dt;
+}
+
+// Plan the next step from the clock and the CFL maximum (run loop of
+// shallow_water_2d.py:402-412): dt = min(cfl_dt, target - t), record when the
+// new time reaches target - 1e-7, stop when all outputs are written or the step
+// cap is reached.
+__device__ inline void plan_next(const DomainDev& d, Control& c) {
+    if (c.idx >= c.n_out || c.steps >= c.max_steps) {
+        c.done = 1;
+        c.snap = -1;
+        return;
+    }
+    if (!(c.maxinv == c.maxinv) || isinf(c.maxinv)) {
+        c.done = 1;
+        c.status = 4;  // SWE_ERR_NONFINITE
+        c.snap = -1;
+        return;
+    }
+    const double target = (double)c.times[c.idx];
+    double dt = cfl_dt_from(d, c.maxinv);
+    const double remain = __dsub_rn(target, c.t);
+    if (remain < dt) dt = remain;
+    c.dt = dt;
+    c.s = step_scalars(d, dt, c.t);
+    c.snap = (__dadd_rn(c.t, dt) >= __dsub_rn(target, 1.0e-7)) ? c.idx : -1;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// NaN-propagating max (np.max semantics).
+__device__ __forceinline__ float nan_max(float a, float b) { return (b > a || b != b) ? b : a; }
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+struct Accum {
+    float maxinv;
+    double vol, rain, outflow, clip, mask;
+    __device__ void zero() { maxinv = 0.f; vol = rain = outflow = clip = mask = 0.0; }
+};
+
+// Reduce per-thread accumulators over the CTA in a fixed order, write the CTA
+// partial, and let the last CTA to finish fold all partials (again in a fixed
+// order, so the ledger is bitwise reproducible) and advance the control block.
+template <int THREADS>
+__device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts, Accum acc,
+                                bool init) {
+    constexpr int W = THREADS / kWarp;
+    __shared__ float s_max[W];
+    __shared__ double s_sum[5][W];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    acc.maxinv = warp_max(acc.maxinv);
+    acc.vol = warp_sum(acc.vol);
+    acc.rain = warp_sum(acc.rain);
+    acc.outflow = warp_sum(acc.outflow);
+    acc.clip = warp_sum(acc.clip);
+    acc.mask = warp_sum(acc.mask);
+    if (lane == 0) {
+        s_max[warp] = acc.maxinv;
+        s_sum[0][warp] = acc.vol;
+        s_sum[1][warp] = acc.rain;
+        s_sum[2][warp] = acc.outflow;
+        s_sum[3][warp] = acc.clip;
+        s_sum[4][warp] = acc.mask;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Partial p;
+        p.maxinv = s_max[0];
+        p.bad = 0;
+        p.vol = s_sum[0][0]; p.rain = s_sum[1][0]; p.outflow = s_sum[2][0];
+        p.clip = s_sum[3][0]; p.mask = s_sum[4][0];
+        for (int w = 1; w < W; ++w) {
+            p.maxinv = nan_max(p.maxinv, s_max[w]);
+            p.vol += s_sum[0][w]; p.rain += s_sum[1][w]; p.outflow += s_sum[2][w];
+            p.clip += s_sum[3][w]; p.mask += s_sum[4][w];
+        }
+        parts[blockIdx.x] = p;
+        __threadfence();
+        const unsigned ticket = atomicAdd(&ctl->counter, 1u);
+        s_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // Fixed-order fold of all CTA partials: thread t folds partials t, t+T, ...
+    Accum a;
+    a.zero();
+    const volatile Partial* vp = parts;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS) {
+        a.maxinv = nan_max(a.maxinv, vp[b].maxinv);
+        a.vol += vp[b].vol; a.rain += vp[b].rain; a.outflow += vp[b].outflow;
+        a.clip += vp[b].clip; a.mask += vp[b].mask;
+    }
+    __syncthreads();
+    a.maxinv = warp_max(a.maxinv);
+    a.vol = warp_sum(a.vol); a.rain = warp_sum(a.rain); a.outflow = warp_sum(a.outflow);
+    a.clip = warp_sum(a.clip); a.mask = warp_sum(a.mask);
+    if (lane == 0) {
+        s_max[warp] = a.maxinv;
+        s_sum[0][warp] = a.vol; s_sum[1][warp] = a.rain; s_sum[2][warp] = a.outflow;
+        s_sum[3][warp] = a.clip; s_sum[4][warp] = a.mask;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    float mx = s_max[0];
+    double vol = s_sum[0][0], rain = s_sum[1][0], outflow = s_sum[2][0], clip = s_sum[3][0],
+           mask = s_sum[4][0];
+    for (int w = 1; w < W; ++w) {
+        mx = nan_max(mx, s_max[w]);
+        vol += s_sum[0][w]; rain += s_sum[1][w]; outflow += s_sum[2][w];
+        clip += s_sum[3][w]; mask += s_sum[4][w];
+    }
+    Control c = *ctl;
+    const double area = d.dx * d.dy;
+    if (init) {
+        c.t = c.t_start;
+        c.idx = 1;
+        c.steps = 0;
+        c.done = 0;
+        c.status = 0;
+        c.ledger[0] = vol * area;
+        c.ledger[1] = vol * area;
+        c.ledger[2] = c.ledger[3] = c.ledger[4] = c.ledger[5] = 0.0;
+    } else {
+        c.t = __dadd_rn(c.t, c.dt);
+        c.steps += 1;
+        if (c.snap >= 0) c.idx = c.snap + 1;
+        c.ledger[1] = vol * area;
+        c.ledger[2] += rain * area;
+        c.ledger[3] += outflow;
+        c.ledger[4] += clip * area;
+        c.ledger[5] += mask * area;
+    }
+    c.maxinv = mx;
+    c.counter = 0;
+    plan_next(d, c);
+    *ctl = c;
+    __threadfence();
+}
+
+// ---------------------------------------------------------------------------
+// The step kernel
+// ---------------------------------------------------------------------------
+struct StepLaunch {
+    DomainDev d;
+    StateView in;
+    StateOut out;
+    StepScalars s;     // used when ctl == nullptr (plain step)
+    Control* ctl;      // run mode when non-null
+    Partial* parts;
+    int nstrips;       // ceil(cols / (32 V))
+    int rows_per_warp;
+};
+
+template <int V, class M, int THREADS, bool RUN>
+__global__ void __launch_bounds__(THREADS) step_kernel(const StepLaunch p) {
+    const DomainDev& d = p.d;
+    const Consts& k = d.k;
+    constexpr bool run = RUN;
+    StepScalars s = p.s;
+    int snap = -1;
+    if (run) {
+        const Control* c = p.ctl;
+        if (*((volatile const int*)&c->done)) return;  // uniform early exit of the whole grid
+        s = c->s;
+        snap = c->snap;
+    }
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (THREADS / kWarp) + (threadIdx.x >> 5);
+    const int strip = gw % p.nstrips;
+    const int chunk = gw / p.nstrips;
+    const int r0 = chunk * p.rows_per_warp;
+    const int r1 = min(r0 + p.rows_per_warp, d.rows);
+    const int x0w = strip * kWarp * V;
+    const int c0 = x0w + lane * V;
+    Accum acc;
+    acc.zero();
+    const double dtd = run ? p.ctl->dt : 0.0;
+
+    if (r0 < d.rows) {
+        Cell cur[V], nxt[V], pre[V];
+        float yT0[V], yT1[V], yT2[V];
+        // Bottom face of the chunk.
+        load_cells<V>(d, p.in, r0 - 1, c0, pre);
+        load_cells<V>(d, p.in, r0, c0, cur);
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            set_vel<M>(pre[i], k.dry);
+            set_vel<M>(cur[i], k.dry);
+            const FaceFlux f = face_flux<0, M>(pre[i], cur[i], k);
+            yT0[i] = f.f0;
+            yT1[i] = f.f1;
+            yT2[i] = M::add(f.f2, f.corr_hi);
+            if (run && r0 == 0 && c0 + i < d.cols) acc.outflow -= dtd * (double)f.f0 * d.dx;
+        }
+        load_cells<V>(d, p.in, r0 + 1, c0, nxt);
+#pragma unroll
+        for (int i = 0; i < V; ++i) set_vel<M>(nxt[i], k.dry);
+
+        for (int r = r0; r < r1; ++r) {
+            // Prefetch the row after next.
+            if (r + 1 < r1) load_cells<V>(d, p.in, r + 2, c0, pre);
+            // Halo cells of row r for the strip edges.
+            Cell lh, rh;
+            if (lane == 0) {
+                Cell t[1];
+                load_cells<1>(d, p.in, r, x0w - 1, t);
+                lh = t[0];
+                set_vel<M>(lh, k.dry);
+            }
+            if (lane == 31) {
+                Cell t[1];
+                load_cells<1>(d, p.in, r, x0w + kWarp * V, t);
+                rh = t[0];
+                set_vel<M>(rh, k.dry);
+            }
+            // y-faces above row r: lo side updates row r, hi side is carried to row r+1.
+            float yB0[V], yB1[V], yB2[V], yN0[V], yN1[V], yN2[V];
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+                const FaceFlux f = face_flux<0, M>(cur[i], nxt[i], k);
+                yB0[i] = f.f0;
+                yB1[i] = f.f1;
+                yB2[i] = M::add(f.f2, f.corr_lo);
+                yN0[i] = f.f0;
+                yN1[i] = f.f1;
+                yN2[i] = M::add(f.f2, f.corr_hi);
+                if (run && r == d.rows - 1 && c0 + i < d.cols) acc.outflow += dtd * (double)f.f0 * d.dx;
+            }
+            // x-faces of row r.  Right neighbour of the last cell of each lane.
+            Cell rn;
+            rn.h = __shfl_down_sync(0xffffffffu, cur[0].h, 1);
+            rn.hu = __shfl_down_sync(0xffffffffu, cur[0].hu, 1);
+            rn.hv = __shfl_down_sync(0xffffffffu, cur[0].hv, 1);
+            rn.z = __shfl_down_sync(0xffffffffu, cur[0].z, 1);
+            rn.nm = __shfl_down_sync(0xffffffffu, cur[0].nm, 1);
+            rn.u = __shfl_down_sync(0xffffffffu, cur[0].u, 1);
+            rn.v = __shfl_down_sync(0xffffffffu, cur[0].v, 1);
+            if (lane == 31) rn = rh;
+            float xl0[V], xl1[V], xl2[V];  // lo-side flux of the right face of cell i
+            float xr0[V], xr1[V], xr2[V];  // hi-side flux of the left face of cell i
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+                const Cell& right = (i + 1 < V) ? cur[(i + 1) % V] : rn;
+                const FaceFlux f = face_flux<1, M>(cur[i], right, k);
+                xl0[i] = f.f0;
+                xl1[i] = M::add(f.f1, f.corr_lo);
+                xl2[i] = f.f2;
+                if (i + 1 < V) {
+                    xr0[(i + 1) % V] = f.f0;
+                    xr1[(i + 1) % V] = M::add(f.f1, f.corr_hi);
+                    xr2[(i + 1) % V] = f.f2;
+                } else {
+                    // hand the hi side to the lane on the right
+                    const float h0 = f.f0, h1 = M::add(f.f1, f.corr_hi), h2 = f.f2;
+                    xr0[0] = __shfl_up_sync(0xffffffffu, h0, 1);
+                    xr1[0] = __shfl_up_sync(0xffffffffu, h1, 1);
+                    xr2[0] = __shfl_up_sync(0xffffffffu, h2, 1);
+                }
+                if (run && c0 + i == d.cols - 1) acc.outflow += dtd * (double)f.f0 * d.dy;
+            }
+            if (lane == 0) {
+                const FaceFlux f = face_flux<1, M>(lh, cur[0], k);
+                xr0[0] = f.f0;
+                xr1[0] = M::add(f.f1, f.corr_hi);
+                xr2[0] = f.f2;
+                if (run && x0w == 0) acc.outflow -= dtd * (double)f.f0 * d.dy;
+            }
+            // Cell updates of row r.
+            const int64_t so = (int64_t)r * p.out.pitch;
+            float ho[V], huo[V], hvo[V];
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+                const bool act = active(cur[i].nm);
+                const float n2 = fabsf(cur[i].nm);
+                float upd[3];
+                const float U[3] = {cur[i].h, cur[i].hu, cur[i].hv};
+                const float XL[3] = {xl0[i], xl1[i], xl2[i]};
+                const float XR[3] = {xr0[i], xr1[i], xr2[i]};
+                const float YB[3] = {yB0[i], yB1[i], yB2[i]};
+                const float YT[3] = {yT0[i], yT1[i], yT2[i]};
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const float divx = M::div(M::sub(XL[q], XR[q]), k.dx);
+                    const float divy = M::div(M::sub(YB[q], YT[q]), k.dy);
+                    upd[q] = M::sub(U[q], M::mul(s.dt, M::add(divx, divy)));
+                }
+                float mult;
+                if (d.mult != nullptr) {
+                    const int cc = min(max(c0 + i, 0), d.cols - 1);
+                    mult = __ldg(d.mult + (int64_t)r * d.spitch + cc);
+                } else {
+                    mult = act ? 1.0f : 0.0f;
+                }
+                const float rain = M::mul(s.dt_rain, mult);
+                upd[0] = M::add(upd[0], rain);
+                const float h = fmaxf(upd[0], 0.0f);
+                const float norm = M::hypot(upd[1], upd[2]);
+                const float fr = M::div(M::mul(M::mul(s.dt_g, n2), norm), M::pow73(fmaxf(h, k.dry), k.expo));
+                const float den = M::add(1.0f, fr);
+                const float qx = M::div(upd[1], den);
+                const float qy = M::div(upd[2], den);
+                const bool wet = act & (h > k.dry);
+                ho[i] = act ? h : 0.0f;
+                huo[i] = wet ? qx : 0.0f;
+                hvo[i] = wet ? qy : 0.0f;
+                if (run && c0 + i < d.cols) {
+                    float u, v;
+                    M::vel2(huo[i], hvo[i], ho[i], k.dry, u, v);
+                    const float w = M::sqrt(M::mul(k.g, ho[i]));
+                    const float inv = M::add(M::div(M::add(fabsf(u), w), k.dx), M::div(M::add(fabsf(v), w), k.dy));
+                    acc.maxinv = nan_max(acc.maxinv, act ? inv : 0.0f);
+                    acc.vol += (double)ho[i];
+                    acc.rain += (double)rain;
+                    if (upd[0] < 0.0f) acc.clip -= (double)upd[0];
+                    if (!act) acc.mask += (double)h;
+                }
+            }
+            // Store row r.
+            if (c0 >= 0 && c0 + V <= d.cols) {
+                if constexpr (V == 4) {
+                    *reinterpret_cast<float4*>(p.out.h + so + c0) = make_float4(ho[0], ho[1], ho[2], ho[3]);
+                    *reinterpret_cast<float4*>(p.out.hu + so + c0) = make_float4(huo[0], huo[1], huo[2], huo[3]);
+                    *reinterpret_cast<float4*>(p.out.hv + so + c0) = make_float4(hvo[0], hvo[1], hvo[2], hvo[3]);
+                } else if constexpr (V == 2) {
+                    *reinterpret_cast<float2*>(p.out.h + so + c0) = make_float2(ho[0], ho[1]);
+                    *reinterpret_cast<float2*>(p.out.hu + so + c0) = make_float2(huo[0], huo[1]);
+                    *reinterpret_cast<float2*>(p.out.hv + so + c0) = make_float2(hvo[0], hvo[1]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < V; ++i) {
+                        p.out.h[so + c0 + i] = ho[i];
+                        p.out.hu[so + c0 + i] = huo[i];
+                        p.out.hv[so + c0 + i] = hvo[i];
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < V; ++i) {
+                    if (c0 + i < d.cols) {
+                        p.out.h[so + c0 + i] = ho[i];
+                        p.out.hu[so + c0 + i] = huo[i];
+                        p.out.hv[so + c0 + i] = hvo[i];
+                    }
+                }
+            }
+            if (snap >= 0) {
+                const Control* c = p.ctl;
+                const int64_t base = (int64_t)snap * c->out_plane + (int64_t)r * d.cols;
+#pragma unroll
+                for (int i = 0; i < V; ++i) {
+                    if (c0 + i < d.cols) {
+                        c->out_h[base + c0 + i] = ho[i];
+                        c->out_hu[base + c0 + i] = huo[i];
+                        c->out_hv[base + c0 + i] = hvo[i];
+                    }
+                }
+            }
+            // Advance: row r+1 becomes current and inherits the carried face values.
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+                yT0[i] = yN0[i];
+                yT1[i] = yN1[i];
+                yT2[i] = yN2[i];
+                cur[i] = nxt[i];
+                nxt[i] = pre[i];
+                set_vel<M>(nxt[i], k.dry);
+            }
+        }
+    }
+    if constexpr (RUN) finish_run_step<THREADS>(d, p.ctl, p.parts, acc, false);
+}
+
+// Max inverse CFL dt and stored volume of a state (the reduction of
+// compute_cfl_dt, shallow_water_2d.py:269-273); initialises the run control.
+template <class M, int THREADS>
+__global__ void __launch_bounds__(THREADS) reduce_kernel(const DomainDev d, const StateView s,
+                                                         Control* ctl, Partial* parts) {
+    const Consts& k = d.k;
+    Accum acc;
+    acc.zero();
+    const int64_t n = (int64_t)d.rows * d.cols;
+    for (int64_t i = (int64_t)blockIdx.x * THREADS + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * THREADS) {
+        const int r = (int)(i / d.cols), c = (int)(i - (int64_t)r * d.cols);
+        const float h = s.h[(int64_t)r * s.pitch + c];
+        const float hu = s.hu[(int64_t)r * s.pitch + c];
+        const float hv = s.hv[(int64_t)r * s.pitch + c];
+        const bool act = active(d.nm[(int64_t)r * d.spitch + c]);
+        float u, v;
+        M::vel2(hu, hv, h, k.dry, u, v);
+        const float w = M::sqrt(M::mul(k.g, fmaxf(h, 0.0f)));
+        const float inv = M::add(M::div(M::add(fabsf(u), w), k.dx), M::div(M::add(fabsf(v), w), k.dy));
+        acc.maxinv = nan_max(acc.maxinv, act ? inv : 0.0f);
+        if (act) acc.vol += (double)h;
+    }
+    finish_run_step<THREADS>(d, ctl, parts, acc, true);
+}
+
+}  // namespace swe

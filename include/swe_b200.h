@@ -1,0 +1,154 @@
+/* swe_b200.h -- C ABI of the B200 (sm_100a) shallow-water finite-volume step.
+ *
+ * Drop-in boundary for the hot path of arsanjeevk/gpu-hybrid-flood-forecasting.
+ * Each entry point replaces one function of the reference (paths inside the
+ * reference project):
+ *
+ *   swe_domain_create   NumpyShallowWaterSolver.__init__ / ShallowWaterSolver.__init__
+ *                       src/hybrid_flood/numpy_solver/shallow_water_2d.py:333-365,
+ *                       src/hybrid_flood/jax_solver/shallow_water_2d.py:213-253
+ *                       (plus boundary codes, jax_solver/boundary_conditions.py:9-26)
+ *   swe_step            finite_volume_step(state, params, dt, time_s)
+ *                       numpy_solver/shallow_water_2d.py:277-327, jax_solver/numerics.py:312-369
+ *   swe_max_inverse_dt  the reduction inside compute_cfl_dt
+ *                       numpy_solver/shallow_water_2d.py:269-273, jax_solver/numerics.py:299-304
+ *   swe_cfl_dt          compute_cfl_dt(state, params)
+ *                       numpy_solver/shallow_water_2d.py:267-274, jax_solver/numerics.py:297-309
+ *   swe_rainfall_rate   rainfall_rate(params, time_s)
+ *                       numpy_solver/shallow_water_2d.py:254-264, jax_solver/numerics.py:286-294
+ *   swe_run             NumpyShallowWaterSolver.run / ShallowWaterSolver.run / integrate_to_outputs
+ *                       numpy_solver/shallow_water_2d.py:382-424,
+ *                       jax_solver/shallow_water_2d.py:278-306, jax_solver/numerics.py:372-434
+ *   swe_advance         the fixed-count step loop of jax_solver/benchmarking.py:46-57,
+ *                       with CFL-limited dt as in the run loop
+ *
+ * Conventions
+ *   - Fields are float32, row-major [rows][cols]: row index = y (northward),
+ *     column = x (eastward).  `pitch` is the row stride in ELEMENTS (>= cols).
+ *   - State and output buffers are caller-owned DEVICE pointers.  Static fields
+ *     passed to swe_domain_create may be host or device pointers (see
+ *     `fields_on_host`); the domain keeps its own packed device copy.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  All work is
+ *     enqueued on it; entry points that return a host value synchronise it.
+ *   - Every entry point returns an int status (SWE_OK = 0).  swe_last_error()
+ *     gives the message of the last failure on the calling thread.
+ *   - A domain handle may be used by one host thread at a time.
+ */
+#ifndef SWE_B200_H
+#define SWE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWE_OK 0
+#define SWE_ERR_INVALID 1   /* bad argument: the reference raises ValueError */
+#define SWE_ERR_CUDA 2      /* CUDA runtime error */
+#define SWE_ERR_MAX_STEPS 3 /* max_steps ran out: the reference raises RuntimeError */
+#define SWE_ERR_NONFINITE 4 /* NaN/Inf reached the CFL reduction */
+#define SWE_ERR_NO_DEVICE 5 /* no usable sm_100 device */
+
+#define SWE_REFLECTIVE 0 /* jax_solver/boundary_conditions.py:9 */
+#define SWE_OPEN 1       /* jax_solver/boundary_conditions.py:10 (zero-gradient copy) */
+
+#define SWE_ARITH_EXACT 0 /* every operation rounded as the reference NumPy solver */
+#define SWE_ARITH_FAST 1  /* FMA + hardware approximations, tolerance-checked */
+
+typedef struct swe_domain *swe_domain_t;
+
+typedef struct {
+    int32_t rows, cols;
+    double dx, dy;             /* cell size (m); the reference uses dx = dy = resolution_m */
+    double gravity;            /* m s^-2, reference default 9.81 */
+    double cfl;                /* reference default 0.45 */
+    double dry_tolerance;      /* m, reference default 1e-4 */
+    double max_dt;             /* s, reference default 10 */
+    double default_rainfall;   /* m/s outside the hyetograph record */
+    int32_t boundary[4];       /* left, right, bottom, top: SWE_REFLECTIVE / SWE_OPEN */
+    int32_t n_rain;            /* hyetograph length (>= 1) */
+    const float *rain_times;   /* HOST, n_rain times (s), increasing */
+    const float *rain_rates;   /* HOST, n_rain rates (m/s) */
+    const float *bed;          /* rows*cols, contiguous */
+    const float *manning_n;    /* rows*cols */
+    const uint8_t *domain_mask;/* rows*cols, nonzero = active */
+    const float *rainfall_multiplier; /* rows*cols, or NULL = domain_mask as 0/1 */
+    int32_t fields_on_host;    /* 1: bed/manning_n/domain_mask/multiplier are host pointers */
+    int32_t arithmetic;        /* SWE_ARITH_EXACT or SWE_ARITH_FAST */
+} swe_domain_desc;
+
+typedef struct {
+    double final_time_s;   /* NumpyResult.final_time_s */
+    int32_t outputs_written;
+    int32_t steps_used;
+    int32_t status;        /* SWE_OK, SWE_ERR_MAX_STEPS or SWE_ERR_NONFINITE */
+    int32_t reserved;
+    /* FP64 mass ledger (m^3): volume0, volume, rain_in, outflow, clip_gain, mask_loss.
+     * volume - (volume0 + rain_in - outflow + clip_gain - mask_loss) is the closing error. */
+    double ledger[6];
+} swe_run_result;
+
+/* Create a domain: validates the descriptor, packs bed and n^2 (with the mask)
+ * into pitched device planes, uploads the hyetograph.  Allocates device memory. */
+int swe_domain_create(const swe_domain_desc *desc, swe_domain_t *out);
+int swe_domain_destroy(swe_domain_t d);
+
+/* One step: out = finite_volume_step(in, params, dt, time_s).  `dt` and
+ * `time_s` are float64 as in the reference; the kernel rounds dt, dt*rate and
+ * dt*gravity to float32 where the reference does.  Outputs must not alias inputs. */
+int swe_step(swe_domain_t d, const float *h, const float *hu, const float *hv, int64_t pitch_in,
+             float *h_out, float *hu_out, float *hv_out, int64_t pitch_out, double dt,
+             double time_s, void *stream);
+
+/* Largest (|u|+c)/dx + (|v|+c)/dy over active cells (float32, as the reference). */
+int swe_max_inverse_dt(swe_domain_t d, const float *h, const float *hu, const float *hv,
+                       int64_t pitch, float *max_inverse_dt_out, void *stream);
+
+/* compute_cfl_dt: min(cfl / max_inverse_dt, max_dt), or max_dt if the maximum is 0. */
+int swe_cfl_dt(swe_domain_t d, const float *h, const float *hu, const float *hv, int64_t pitch,
+               double *dt_out, void *stream);
+
+/* rainfall_rate: np.interp of the hyetograph at time_s (float64). */
+int swe_rainfall_rate(swe_domain_t d, double time_s, double *rate_out);
+
+/* Adaptive run to fixed output times (the reference run loop: dt = min(cfl_dt,
+ * target - t), an output is recorded when t >= target - 1e-7).  The clock is
+ * float64 and lives on the device; the host only polls completion.
+ *   output_times: HOST float32[n_out], output_times[0] == 0, strictly increasing
+ *   out_*: DEVICE float32[n_out][rows][cols] (slot 0 receives the initial state)
+ * Returns SWE_ERR_MAX_STEPS (result filled) when max_steps was insufficient. */
+int swe_run(swe_domain_t d, const float *h0, const float *hu0, const float *hv0,
+            int64_t pitch_in, const float *output_times, int32_t n_out, int32_t max_steps,
+            float *out_h, float *out_hu, float *out_hv, swe_run_result *result, void *stream);
+
+/* Advance (h, hu, hv) in place by exactly n_steps CFL-limited steps starting at
+ * time start_s; the state, final time and ledger are returned in `result`. */
+int swe_advance(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, int32_t n_steps,
+                double start_s, swe_run_result *result, void *stream);
+
+/* Number of kernel launches the last swe_run/swe_advance on this domain enqueued. */
+int64_t swe_last_launch_count(swe_domain_t d);
+
+/* Enable (1) or disable (0) CUDA-event timing of the step kernels that
+ * swe_run/swe_advance enqueue (events on the caller's stream around the first
+ * and the last step launch). */
+int swe_set_timing(swe_domain_t d, int32_t enable);
+
+/* Milliseconds between the start of the first and the end of the last step
+ * kernel of the last timed swe_run/swe_advance, and the step launches between. */
+int swe_last_step_time(swe_domain_t d, double *ms, int64_t *step_launches);
+
+/* Copy the message of the last error on this thread into buf (NUL-terminated);
+ * returns the full message length. */
+int swe_last_error(char *buf, size_t n);
+
+/* Library version string, e.g. "swe_b200 0.1.0 sm_100a". */
+const char *swe_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SWE_B200_H */
