@@ -101,51 +101,79 @@ struct swe_domain {
     int64_t timed_steps = 0;
     int64_t launches = 0;
     int rows_per_warp_override = 0;
+    int run_vec = 2;     // vector width of the run-mode kernel (SWE_RUN_VEC=1|2|4)
+    bool masked = true;  // false when every cell is active (mask-free kernels)
 };
 
 namespace {
 
-Plan make_plan(const swe_domain* d, int V) {
+// Kernel instance for (vector width, arithmetic, run mode, masked) chosen at run time.
+template <int V, class M, bool RUN, bool MASKED>
+struct StepK {
+    static const void* fn() { return reinterpret_cast<const void*>(&step_kernel<V, M, kThreads, RUN, MASKED>); }
+    static void launch(int blocks, const StepLaunch& sl, cudaStream_t st) {
+        step_kernel<V, M, kThreads, RUN, MASKED><<<blocks, kThreads, 0, st>>>(sl);
+    }
+};
+
+template <class M, bool RUN, bool MASKED, class F>
+void dispatch_v(int V, F&& f) {
+    switch (V) {
+        case 4: f(StepK<4, M, RUN, MASKED>{}); break;
+        case 2: f(StepK<2, M, RUN, MASKED>{}); break;
+        default: f(StepK<1, M, RUN, MASKED>{}); break;
+    }
+}
+
+template <class F>
+void dispatch(int V, int arith, bool run, bool masked, F&& f) {
+    if (arith == SWE_ARITH_FAST) {
+        if (run) {
+            if (masked) dispatch_v<FastMath, true, true>(V, f); else dispatch_v<FastMath, true, false>(V, f);
+        } else {
+            if (masked) dispatch_v<FastMath, false, true>(V, f); else dispatch_v<FastMath, false, false>(V, f);
+        }
+    } else {
+        if (run) {
+            if (masked) dispatch_v<ExactMath, true, true>(V, f); else dispatch_v<ExactMath, true, false>(V, f);
+        } else {
+            if (masked) dispatch_v<ExactMath, false, true>(V, f); else dispatch_v<ExactMath, false, false>(V, f);
+        }
+    }
+}
+
+// Work items are (strip of 32*V columns) x (chunk of R rows), one per warp.  R is
+// chosen so that all warps are resident at once (one full wave at the kernel's
+// occupancy), which equalises the work of every SM; chunks keep >= 4 rows.
+Plan make_plan(const swe_domain* d, int V, bool run) {
     Plan p;
     p.V = V;
     const int rows = d->dd.rows, cols = d->dd.cols;
     p.nstrips = (cols + kWarp * V - 1) / (kWarp * V);
+    int occ = 1;
+    dispatch(V, d->arith, run, d->masked, [&](auto k) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, decltype(k)::fn(), kThreads, 0) == cudaSuccess && n > 0)
+            occ = n;
+    });
+    const int wpb = kThreads / kWarp;
+    const int64_t warps_avail = (int64_t)occ * d->sms * wpb;
     int R = d->rows_per_warp_override;
     if (R <= 0) {
-        // Aim for ~32 resident warps per SM worth of work items, chunks of >= 8 rows.
-        const int64_t target = (int64_t)d->sms * 32;
-        R = (int)((int64_t)rows * p.nstrips / std::max<int64_t>(target, 1));
-        R = std::max(8, std::min(R, 64));
+        const int64_t chunks = std::max<int64_t>(1, warps_avail / p.nstrips);
+        R = (int)((rows + chunks - 1) / chunks);
+        R = std::max(R, std::min(4, rows));
     }
     p.rows_per_warp = R;
     const int64_t chunks = (rows + R - 1) / R;
     const int64_t warps = chunks * p.nstrips;
-    const int wpb = kThreads / kWarp;
     p.blocks = (int)((warps + wpb - 1) / wpb);
     return p;
 }
 
-template <int V, class M, bool RUN>
-void launch_step_t(const Plan& pl, const StepLaunch& sl, cudaStream_t st) {
-    step_kernel<V, M, kThreads, RUN><<<pl.blocks, kThreads, 0, st>>>(sl);
-}
-
-template <class M, bool RUN>
-void launch_step_m(const Plan& pl, const StepLaunch& sl, cudaStream_t st) {
-    switch (pl.V) {
-        case 4: launch_step_t<4, M, RUN>(pl, sl, st); break;
-        case 2: launch_step_t<2, M, RUN>(pl, sl, st); break;
-        default: launch_step_t<1, M, RUN>(pl, sl, st); break;
-    }
-}
-
 void launch_step(const swe_domain* d, const Plan& pl, const StepLaunch& sl, bool run,
                  cudaStream_t st) {
-    if (d->arith == SWE_ARITH_FAST) {
-        if (run) launch_step_m<FastMath, true>(pl, sl, st); else launch_step_m<FastMath, false>(pl, sl, st);
-    } else {
-        if (run) launch_step_m<ExactMath, true>(pl, sl, st); else launch_step_m<ExactMath, false>(pl, sl, st);
-    }
+    dispatch(pl.V, d->arith, run, d->masked, [&](auto k) { decltype(k)::launch(pl.blocks, sl, st); });
 }
 
 int reduce_blocks(const swe_domain* d) {
@@ -214,7 +242,7 @@ int run_driver(swe_domain* d, StateView init, const float* times_host, int n_tim
     const int rows = d->dd.rows, cols = d->dd.cols;
     int rc = ensure_ping(d);
     if (rc) return rc;
-    const Plan pl = make_plan(d, 2);
+    const Plan pl = make_plan(d, d->run_vec, true);
     rc = ensure_parts(d, std::max(pl.blocks, reduce_blocks(d)));
     if (rc) return rc;
     for (int f = 0; f < 3; ++f) {
@@ -329,7 +357,7 @@ void free_domain(swe_domain* d) {
 
 __global__ void pack_static_kernel(const float* bed, const float* man, const uint8_t* mask,
                                    const float* mult, int rows, int cols, int64_t pitch,
-                                   float* bed_o, float* nm_o, float* mult_o) {
+                                   float* bed_o, float* nm_o, float* mult_o, int* any_inactive) {
     const int64_t n = (int64_t)rows * pitch;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -342,6 +370,7 @@ __global__ void pack_static_kernel(const float* bed, const float* man, const uin
         bed_o[i] = bed[j];
         // The domain mask rides in the sign bit: set = inactive.
         nm_o[i] = mask[j] ? n2a : __int_as_float(__float_as_int(n2a) | (int)0x80000000);
+        if (!mask[j]) *any_inactive = 1;
         if (mult_o) mult_o[i] = mult[j];
     }
 }
@@ -390,6 +419,10 @@ int swe_domain_create(const swe_domain_desc* desc, swe_domain_t* out) {
     d->sms = prop.multiProcessorCount;
     d->arith = q.arithmetic;
     if (const char* e = std::getenv("SWE_ROWS_PER_WARP")) d->rows_per_warp_override = std::atoi(e);
+    if (const char* e = std::getenv("SWE_RUN_VEC")) {
+        const int v = std::atoi(e);
+        if (v == 1 || v == 2 || v == 4) d->run_vec = v;
+    }
     const int rows = q.rows, cols = q.cols;
     const int64_t pitch = round_up(cols, 32);
     const size_t plane = sizeof(float) * (size_t)pitch * rows;
@@ -427,10 +460,16 @@ int swe_domain_create(const swe_domain_desc* desc, swe_domain_t* out) {
         SWE_CK2(cudaMemcpy(p, q.domain_mask, n, cudaMemcpyHostToDevice));
         mask_s = reinterpret_cast<const uint8_t*>(p);
     }
+    int* flag = nullptr;
+    SWE_CK2(cudaMalloc(&flag, sizeof(int)));
+    SWE_CK2(cudaMemset(flag, 0, sizeof(int)));
     pack_static_kernel<<<std::min<int64_t>((rows * pitch + 255) / 256, 4096), 256>>>(
-        bed_s, man_s, mask_s, mult_s, rows, cols, pitch, d->bed, d->nm, d->mult);
+        bed_s, man_s, mask_s, mult_s, rows, cols, pitch, d->bed, d->nm, d->mult, flag);
     SWE_CK2(cudaGetLastError());
-    SWE_CK2(cudaDeviceSynchronize());
+    int any_inactive = 1;
+    SWE_CK2(cudaMemcpy(&any_inactive, flag, sizeof(int), cudaMemcpyDeviceToHost));
+    cudaFree(flag);
+    d->masked = any_inactive != 0;
     if (staging) cudaFree(staging);
     // Hyetograph as float64 (np.interp converts the float32 table to float64).
     d->rain_t.resize(q.n_rain);
@@ -507,7 +546,7 @@ int swe_step(swe_domain_t d, const float* h, const float* hu, const float* hv, i
             if (a == b) return fail(SWE_ERR_INVALID, "step outputs must not alias its inputs");
     const void* all[6] = {h, hu, hv, h_out, hu_out, hv_out};
     const int V = choose_vec(all, 6, pitch_in, pitch_out);
-    const Plan pl = make_plan(d, V);
+    const Plan pl = make_plan(d, V, false);
     const double rate = host_rain_rate(d->rain_t, d->rain_r, d->dd.default_rain, time_s);
     StepLaunch sl{};
     sl.d = d->dd;

@@ -183,9 +183,10 @@ struct FaceFlux {
 };
 
 // AXIS 1: x-face (normal momentum hu), AXIS 0: y-face (normal momentum hv).
-template <int AXIS, class M>
+template <int AXIS, class M, bool MASKED = true>
 __device__ __forceinline__ FaceFlux face_flux(const Cell& lo, const Cell& hi, const Consts& k) {
-    const bool a_lo = active(lo.nm), a_hi = active(hi.nm);
+    // Without a domain mask every cell is active: no walls, every face relevant.
+    const bool a_lo = MASKED ? active(lo.nm) : true, a_hi = MASKED ? active(hi.nm) : true;
     const bool relevant = a_lo | a_hi;
     const bool hi_wall = a_lo & !a_hi;  // mirror lo onto hi
     const bool lo_wall = !a_lo & a_hi;  // mirror hi onto lo
@@ -325,6 +326,8 @@ __device__ inline void plan_next(const DomainDev& d, Control& c) {
     c.dt = dt;
     c.s = step_scalars(d, dt, c.t);
     c.snap = (__dadd_rn(c.t, dt) >= __dsub_rn(target, 1.0e-7)) ? c.idx : -1;
+    // Without output buffers (fixed-count advance) nothing is recorded.
+    if (c.out_h == nullptr) c.snap = -1;
 }
 
 template <typename T>
@@ -347,6 +350,25 @@ struct Accum {
     float maxinv;
     double vol, rain, outflow, clip, mask;
     __device__ void zero() { maxinv = 0.f; vol = rain = outflow = clip = mask = 0.0; }
+};
+
+// Per-thread accumulators of the step kernel.  Without a rain-multiplier plane
+// every active cell receives the same float32 increment, so the rain term is
+// kept as a cell count and multiplied out once per thread.
+// Stored volume is summed in float64 per cell; the other terms (edge fluxes,
+// positivity-clip and masked-cell corrections) are a few small values per
+// thread and are summed in float32 before the float64 reduction across threads.
+struct StepAccum {
+    float maxinv;
+    unsigned rain_cells;
+    double vol;
+    float rain, outflow, clip, mask;
+    __device__ void zero() {
+        maxinv = 0.f;
+        rain_cells = 0u;
+        vol = 0.0;
+        rain = outflow = clip = mask = 0.f;
+    }
 };
 
 // Reduce per-thread accumulators over the CTA in a fixed order, write the CTA
@@ -464,82 +486,110 @@ struct StepLaunch {
     int rows_per_warp;
 };
 
-template <int V, class M, int THREADS, bool RUN>
-__global__ void __launch_bounds__(THREADS) step_kernel(const StepLaunch p) {
+// Resident CTAs per SM the register budget is capped for (V=2: 128 registers).
+template <int V>
+struct MinBlocks {
+    static constexpr int value = V == 1 ? 4 : (V == 2 ? 4 : 2);
+};
+
+template <int V, class M, int THREADS, bool RUN, bool MASKED>
+__global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(const StepLaunch p) {
+    constexpr int NW = THREADS / kWarp;
+    constexpr int kBatch = kWarp;  // strip-edge work is done for 32 rows at a time
+    // Warp-private staging of the strip edges for the current batch of rows:
+    // hi side of the strip's left x-face, and the cell right of the strip.
+    __shared__ float s_left[NW][3][kBatch];
+    __shared__ float s_right[NW][7][kBatch];
+
     const DomainDev& d = p.d;
     const Consts& k = d.k;
     constexpr bool run = RUN;
     StepScalars s = p.s;
     int snap = -1;
-    if (run) {
+    double dtd = 0.0;
+    if constexpr (RUN) {
         const Control* c = p.ctl;
         if (*((volatile const int*)&c->done)) return;  // uniform early exit of the whole grid
         s = c->s;
         snap = c->snap;
+        dtd = c->dt;
     }
     const int lane = threadIdx.x & 31;
-    const int gw = blockIdx.x * (THREADS / kWarp) + (threadIdx.x >> 5);
+    const int wib = threadIdx.x >> 5;
+    const int gw = blockIdx.x * NW + wib;
     const int strip = gw % p.nstrips;
     const int chunk = gw / p.nstrips;
     const int r0 = chunk * p.rows_per_warp;
     const int r1 = min(r0 + p.rows_per_warp, d.rows);
     const int x0w = strip * kWarp * V;
     const int c0 = x0w + lane * V;
-    Accum acc;
+    StepAccum acc;
     acc.zero();
-    const double dtd = run ? p.ctl->dt : 0.0;
 
     if (r0 < d.rows) {
-        Cell cur[V], nxt[V], pre[V];
+        Cell A[V], B[V], C[V];
         float yT0[V], yT1[V], yT2[V];
-        // Bottom face of the chunk.
-        load_cells<V>(d, p.in, r0 - 1, c0, pre);
-        load_cells<V>(d, p.in, r0, c0, cur);
+        // Bottom face of the chunk: rows r0-1 (A) and r0 (B).
+        load_cells<V>(d, p.in, r0 - 1, c0, A);
+        load_cells<V>(d, p.in, r0, c0, B);
 #pragma unroll
         for (int i = 0; i < V; ++i) {
-            set_vel<M>(pre[i], k.dry);
-            set_vel<M>(cur[i], k.dry);
-            const FaceFlux f = face_flux<0, M>(pre[i], cur[i], k);
+            set_vel<M>(A[i], k.dry);
+            set_vel<M>(B[i], k.dry);
+            const FaceFlux f = face_flux<0, M, MASKED>(A[i], B[i], k);
             yT0[i] = f.f0;
             yT1[i] = f.f1;
             yT2[i] = M::add(f.f2, f.corr_hi);
-            if (run && r0 == 0 && c0 + i < d.cols) acc.outflow -= dtd * (double)f.f0 * d.dx;
+            if (run && r0 == 0 && c0 + i < d.cols) acc.outflow -= (float)(dtd * (double)f.f0 * d.dx);
         }
-        load_cells<V>(d, p.in, r0 + 1, c0, nxt);
+        load_cells<V>(d, p.in, r0 + 1, c0, C);
 #pragma unroll
-        for (int i = 0; i < V; ++i) set_vel<M>(nxt[i], k.dry);
+        for (int i = 0; i < V; ++i) set_vel<M>(C[i], k.dry);
 
-        for (int r = r0; r < r1; ++r) {
+        // One row: `cur` is row r, `nxt` row r+1 (velocities set); `pre` receives row r+2.
+        auto row = [&](const int r, Cell(&cur)[V], Cell(&nxt)[V], Cell(&pre)[V]) {
+            const int j = (r - r0) & (kBatch - 1);
+            if (j == 0) {
+                // Strip edges for rows r .. r+31, one row per lane.
+                __syncwarp();
+                const int rr = min(r + lane, d.rows - 1);
+                Cell L[1], E[1], R[1];
+                load_cells<1>(d, p.in, rr, x0w - 1, L);
+                load_cells<1>(d, p.in, rr, x0w, E);
+                load_cells<1>(d, p.in, rr, x0w + kWarp * V, R);
+                set_vel<M>(L[0], k.dry);
+                set_vel<M>(E[0], k.dry);
+                set_vel<M>(R[0], k.dry);
+                const FaceFlux f = face_flux<1, M, MASKED>(L[0], E[0], k);
+                s_left[wib][0][lane] = f.f0;
+                s_left[wib][1][lane] = M::add(f.f1, f.corr_hi);
+                s_left[wib][2][lane] = f.f2;
+                if (run && x0w == 0 && r + lane < r1) acc.outflow -= (float)(dtd * (double)f.f0 * d.dy);
+                s_right[wib][0][lane] = R[0].h;
+                s_right[wib][1][lane] = R[0].hu;
+                s_right[wib][2][lane] = R[0].hv;
+                s_right[wib][3][lane] = R[0].z;
+                s_right[wib][4][lane] = R[0].nm;
+                s_right[wib][5][lane] = R[0].u;
+                s_right[wib][6][lane] = R[0].v;
+                __syncwarp();
+            }
             // Prefetch the row after next.
             if (r + 1 < r1) load_cells<V>(d, p.in, r + 2, c0, pre);
-            // Halo cells of row r for the strip edges.
-            Cell lh, rh;
-            if (lane == 0) {
-                Cell t[1];
-                load_cells<1>(d, p.in, r, x0w - 1, t);
-                lh = t[0];
-                set_vel<M>(lh, k.dry);
-            }
-            if (lane == 31) {
-                Cell t[1];
-                load_cells<1>(d, p.in, r, x0w + kWarp * V, t);
-                rh = t[0];
-                set_vel<M>(rh, k.dry);
-            }
             // y-faces above row r: lo side updates row r, hi side is carried to row r+1.
             float yB0[V], yB1[V], yB2[V], yN0[V], yN1[V], yN2[V];
 #pragma unroll
             for (int i = 0; i < V; ++i) {
-                const FaceFlux f = face_flux<0, M>(cur[i], nxt[i], k);
+                const FaceFlux f = face_flux<0, M, MASKED>(cur[i], nxt[i], k);
                 yB0[i] = f.f0;
                 yB1[i] = f.f1;
                 yB2[i] = M::add(f.f2, f.corr_lo);
                 yN0[i] = f.f0;
                 yN1[i] = f.f1;
                 yN2[i] = M::add(f.f2, f.corr_hi);
-                if (run && r == d.rows - 1 && c0 + i < d.cols) acc.outflow += dtd * (double)f.f0 * d.dx;
+                if (run && r == d.rows - 1 && c0 + i < d.cols) acc.outflow += (float)(dtd * (double)f.f0 * d.dx);
             }
-            // x-faces of row r.  Right neighbour of the last cell of each lane.
+            // x-faces of row r: right neighbour of each lane's last cell.
             Cell rn;
             rn.h = __shfl_down_sync(0xffffffffu, cur[0].h, 1);
             rn.hu = __shfl_down_sync(0xffffffffu, cur[0].hu, 1);
@@ -548,13 +598,18 @@ __global__ void __launch_bounds__(THREADS) step_kernel(const StepLaunch p) {
             rn.nm = __shfl_down_sync(0xffffffffu, cur[0].nm, 1);
             rn.u = __shfl_down_sync(0xffffffffu, cur[0].u, 1);
             rn.v = __shfl_down_sync(0xffffffffu, cur[0].v, 1);
-            if (lane == 31) rn = rh;
-            float xl0[V], xl1[V], xl2[V];  // lo-side flux of the right face of cell i
-            float xr0[V], xr1[V], xr2[V];  // hi-side flux of the left face of cell i
+            {
+                const float e0 = s_right[wib][0][j], e1 = s_right[wib][1][j], e2 = s_right[wib][2][j];
+                const float e3 = s_right[wib][3][j], e4 = s_right[wib][4][j], e5 = s_right[wib][5][j];
+                const float e6 = s_right[wib][6][j];
+                if (lane == 31) rn = Cell{e0, e1, e2, e3, e4, e5, e6};
+            }
+            float xl0[V], xl1[V], xl2[V];  // lo side of the right face of cell i
+            float xr0[V], xr1[V], xr2[V];  // hi side of the left face of cell i
 #pragma unroll
             for (int i = 0; i < V; ++i) {
                 const Cell& right = (i + 1 < V) ? cur[(i + 1) % V] : rn;
-                const FaceFlux f = face_flux<1, M>(cur[i], right, k);
+                const FaceFlux f = face_flux<1, M, MASKED>(cur[i], right, k);
                 xl0[i] = f.f0;
                 xl1[i] = M::add(f.f1, f.corr_lo);
                 xl2[i] = f.f2;
@@ -563,28 +618,28 @@ __global__ void __launch_bounds__(THREADS) step_kernel(const StepLaunch p) {
                     xr1[(i + 1) % V] = M::add(f.f1, f.corr_hi);
                     xr2[(i + 1) % V] = f.f2;
                 } else {
-                    // hand the hi side to the lane on the right
                     const float h0 = f.f0, h1 = M::add(f.f1, f.corr_hi), h2 = f.f2;
                     xr0[0] = __shfl_up_sync(0xffffffffu, h0, 1);
                     xr1[0] = __shfl_up_sync(0xffffffffu, h1, 1);
                     xr2[0] = __shfl_up_sync(0xffffffffu, h2, 1);
                 }
-                if (run && c0 + i == d.cols - 1) acc.outflow += dtd * (double)f.f0 * d.dy;
+                if (run && c0 + i == d.cols - 1) acc.outflow += (float)(dtd * (double)f.f0 * d.dy);
             }
-            if (lane == 0) {
-                const FaceFlux f = face_flux<1, M>(lh, cur[0], k);
-                xr0[0] = f.f0;
-                xr1[0] = M::add(f.f1, f.corr_hi);
-                xr2[0] = f.f2;
-                if (run && x0w == 0) acc.outflow -= dtd * (double)f.f0 * d.dy;
+            {
+                const float l0 = s_left[wib][0][j], l1 = s_left[wib][1][j], l2 = s_left[wib][2][j];
+                if (lane == 0) {
+                    xr0[0] = l0;
+                    xr1[0] = l1;
+                    xr2[0] = l2;
+                }
             }
             // Cell updates of row r.
             const int64_t so = (int64_t)r * p.out.pitch;
             float ho[V], huo[V], hvo[V];
 #pragma unroll
             for (int i = 0; i < V; ++i) {
-                const bool act = active(cur[i].nm);
-                const float n2 = fabsf(cur[i].nm);
+                const bool act = MASKED ? active(cur[i].nm) : true;
+                const float n2 = MASKED ? fabsf(cur[i].nm) : cur[i].nm;
                 float upd[3];
                 const float U[3] = {cur[i].h, cur[i].hu, cur[i].hv};
                 const float XL[3] = {xl0[i], xl1[i], xl2[i]};
@@ -597,14 +652,13 @@ __global__ void __launch_bounds__(THREADS) step_kernel(const StepLaunch p) {
                     const float divy = M::div(M::sub(YB[q], YT[q]), k.dy);
                     upd[q] = M::sub(U[q], M::mul(s.dt, M::add(divx, divy)));
                 }
-                float mult;
+                float rain;
                 if (d.mult != nullptr) {
                     const int cc = min(max(c0 + i, 0), d.cols - 1);
-                    mult = __ldg(d.mult + (int64_t)r * d.spitch + cc);
+                    rain = M::mul(s.dt_rain, __ldg(d.mult + (int64_t)r * d.spitch + cc));
                 } else {
-                    mult = act ? 1.0f : 0.0f;
+                    rain = act ? s.dt_rain : 0.0f;  // float(dt*rate) * 1.0 or * 0.0
                 }
-                const float rain = M::mul(s.dt_rain, mult);
                 upd[0] = M::add(upd[0], rain);
                 const float h = fmaxf(upd[0], 0.0f);
                 const float norm = M::hypot(upd[1], upd[2]);
@@ -623,13 +677,13 @@ __global__ void __launch_bounds__(THREADS) step_kernel(const StepLaunch p) {
                     const float inv = M::add(M::div(M::add(fabsf(u), w), k.dx), M::div(M::add(fabsf(v), w), k.dy));
                     acc.maxinv = nan_max(acc.maxinv, act ? inv : 0.0f);
                     acc.vol += (double)ho[i];
-                    acc.rain += (double)rain;
-                    if (upd[0] < 0.0f) acc.clip -= (double)upd[0];
-                    if (!act) acc.mask += (double)h;
+                    if (d.mult != nullptr) acc.rain += rain; else acc.rain_cells += act ? 1u : 0u;
+                    if (upd[0] < 0.0f) acc.clip -= upd[0];
+                    if (MASKED && !act) acc.mask += h;
                 }
             }
             // Store row r.
-            if (c0 >= 0 && c0 + V <= d.cols) {
+            if (c0 + V <= d.cols) {
                 if constexpr (V == 4) {
                     *reinterpret_cast<float4*>(p.out.h + so + c0) = make_float4(ho[0], ho[1], ho[2], ho[3]);
                     *reinterpret_cast<float4*>(p.out.hu + so + c0) = make_float4(huo[0], huo[1], huo[2], huo[3]);
@@ -656,7 +710,7 @@ __global__ void __launch_bounds__(THREADS) step_kernel(const StepLaunch p) {
                     }
                 }
             }
-            if (snap >= 0) {
+            if (RUN && snap >= 0) {
                 const Control* c = p.ctl;
                 const int64_t base = (int64_t)snap * c->out_plane + (int64_t)r * d.cols;
 #pragma unroll
@@ -668,19 +722,33 @@ __global__ void __launch_bounds__(THREADS) step_kernel(const StepLaunch p) {
                     }
                 }
             }
-            // Advance: row r+1 becomes current and inherits the carried face values.
+            // Row r+1 inherits the carried face values; the prefetched row gets velocities.
 #pragma unroll
             for (int i = 0; i < V; ++i) {
                 yT0[i] = yN0[i];
                 yT1[i] = yN1[i];
                 yT2[i] = yN2[i];
-                cur[i] = nxt[i];
-                nxt[i] = pre[i];
-                set_vel<M>(nxt[i], k.dry);
+                if (r + 1 < r1) set_vel<M>(pre[i], k.dry);
             }
+        };
+
+        // Three-way rotation of the row buffers avoids copying them every row.
+        for (int r = r0; r < r1; r += 3) {
+            row(r, B, C, A);
+            if (r + 1 < r1) row(r + 1, C, A, B);
+            if (r + 2 < r1) row(r + 2, A, B, C);
         }
     }
-    if constexpr (RUN) finish_run_step<THREADS>(d, p.ctl, p.parts, acc, false);
+    if constexpr (RUN) {
+        Accum a;
+        a.maxinv = acc.maxinv;
+        a.vol = acc.vol;
+        a.rain = (double)acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
+        a.outflow = (double)acc.outflow;
+        a.clip = (double)acc.clip;
+        a.mask = (double)acc.mask;
+        finish_run_step<THREADS>(d, p.ctl, p.parts, a, false);
+    }
 }
 
 // Max inverse CFL dt and stored volume of a state (the reduction of
