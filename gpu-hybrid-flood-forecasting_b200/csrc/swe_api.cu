@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -377,6 +378,104 @@ __global__ void pack_static_kernel(const float* bed, const float* man, const uin
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Allocation-free CFL reduction (swe_max_inverse_dt_noalloc)
+// ---------------------------------------------------------------------------
+// Some callers cannot call cudaMalloc at the point where they need a CFL time
+// step: code that runs under a framework's caching allocator (PyTorch's holds
+// the device memory it has reserved, so a direct cudaMalloc can fail although
+// the pool has room), and time-stepping loops that forbid allocation once they
+// are running.  For them this variant of the CFL reduction takes every input
+// and the output from the caller and keeps its scratch -- one partial maximum
+// per CTA and the last-CTA ticket -- in a fixed file-scope device array, so it
+// allocates nothing.  The array is loaded with the library on every GPU that
+// uses it and stays until the process exits.
+namespace {
+
+constexpr int kNoAllocThreads = 256;
+constexpr int kNoAllocCellsPerBlock = 2048;  // 8 cells per thread
+constexpr int kNoAllocMaxBlocks = SWE_NOALLOC_MAX_CELLS / kNoAllocCellsPerBlock;
+constexpr int kNoAllocMaxDevices = 64;
+static_assert(SWE_NOALLOC_MAX_CELLS % kNoAllocCellsPerBlock == 0, "limit must be whole CTAs");
+
+struct NoAllocScratch {
+    float block_max[kNoAllocMaxBlocks];  // 32 KiB of per-CTA partial maxima
+    unsigned ticket;                     // last-CTA counter, zero between calls
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+__global__ void __launch_bounds__(kNoAllocThreads)
+max_inverse_dt_noalloc_kernel(const float* __restrict__ h, const float* __restrict__ hu,
+                              const float* __restrict__ hv, int64_t pitch,
+                              const uint8_t* __restrict__ mask, int rows, int cols, Consts k,
+                              NoAllocScratch* scratch, float* out) {
+    __shared__ float s_max[kNoAllocThreads / kWarp];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t n = (int64_t)rows * cols;
+    const int64_t base = (int64_t)blockIdx.x * kNoAllocCellsPerBlock;
+    float m = 0.f;
+    for (int q = threadIdx.x; q < kNoAllocCellsPerBlock; q += kNoAllocThreads) {
+        const int64_t i = base + q;
+        if (i >= n) break;
+        const int r = (int)(i / cols), c = (int)(i - (int64_t)r * cols);
+        const int64_t o = (int64_t)r * pitch + c;
+        float u, v;
+        const float hh = h[o];
+        ExactMath::vel2(hu[o], hv[o], hh, k.dry, u, v);
+        const float w = ExactMath::sqrt(ExactMath::mul(k.g, fmaxf(hh, 0.0f)));
+        const float inv = ExactMath::add(ExactMath::div(ExactMath::add(fabsf(u), w), k.dx),
+                                         ExactMath::div(ExactMath::add(fabsf(v), w), k.dy));
+        m = nan_max(m, mask[i] ? inv : 0.0f);
+    }
+    m = warp_max(m);
+    if (lane == 0) s_max[warp] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float b = s_max[0];
+        for (int w = 1; w < kNoAllocThreads / kWarp; ++w) b = nan_max(b, s_max[w]);
+        scratch->block_max[blockIdx.x] = b;
+        __threadfence();
+        s_last = atomicAdd(&scratch->ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const volatile float* bm = scratch->block_max;
+    float a = 0.f;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += kNoAllocThreads) a = nan_max(a, bm[b]);
+    a = warp_max(a);
+    __syncthreads();
+    if (lane == 0) s_max[warp] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r = s_max[0];
+        for (int w = 1; w < kNoAllocThreads / kWarp; ++w) r = nan_max(r, s_max[w]);
+        *out = r;
+        scratch->ticket = 0u;  // leave the counter at zero for the next call
+    }
+}
+
+// Device address of g_noalloc_scratch, looked up once per device.
+int noalloc_scratch(NoAllocScratch** out) {
+    static std::mutex mu;
+    static NoAllocScratch* addr[kNoAllocMaxDevices] = {};
+    int dev = 0;
+    SWE_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(SWE_ERR_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        SWE_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        addr[dev] = static_cast<NoAllocScratch*>(p);
+    }
+    *out = addr[dev];
+    return SWE_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* swe_version(void) { return "swe_b200 0.1.0 sm_100a"; }
@@ -657,6 +756,46 @@ int swe_advance(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, i
 }
 
 int64_t swe_last_launch_count(swe_domain_t d) { return d ? d->launches : -1; }
+
+int swe_max_inverse_dt_noalloc(const float* h, const float* hu, const float* hv, int64_t pitch,
+                               const uint8_t* domain_mask, int32_t rows, int32_t cols,
+                               double gravity, double dry_tolerance, double dx, double dy,
+                               float* max_inverse_dt_out, void* stream) {
+    if (!h || !hu || !hv || !domain_mask || !max_inverse_dt_out)
+        return fail(SWE_ERR_INVALID, "null argument");
+    if (rows < 1 || cols < 1) return fail(SWE_ERR_INVALID, "rows and cols must be >= 1");
+    if (pitch < cols) return fail(SWE_ERR_INVALID, "pitch must be >= cols");
+    if (!(dx > 0) || !(dy > 0)) return fail(SWE_ERR_INVALID, "dx and dy must be positive");
+    const int64_t n = (int64_t)rows * cols;
+    if (n > SWE_NOALLOC_MAX_CELLS) {
+        char msg[192];
+        std::snprintf(msg, sizeof msg,
+                      "rows*cols = %lld exceeds the allocation-free limit of %d cells; "
+                      "use swe_max_inverse_dt with a domain instead",
+                      (long long)n, SWE_NOALLOC_MAX_CELLS);
+        return fail(SWE_ERR_INVALID, msg);
+    }
+    NoAllocScratch* scratch = nullptr;
+    const int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    Consts k{};
+    k.g = (float)gravity;
+    k.half_g = (float)(0.5 * gravity);
+    k.dry = (float)dry_tolerance;
+    k.dx = (float)dx;
+    k.dy = (float)dy;
+    k.eps = (float)1.0e-12;
+    k.expo = (float)(7.0 / 3.0);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // The ticket must start at zero; clear it in case an earlier launch was cut short.
+    SWE_CK(cudaMemsetAsync(&scratch->ticket, 0, sizeof(unsigned), st));
+    const int blocks = (int)((n + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock);
+    max_inverse_dt_noalloc_kernel<<<blocks, kNoAllocThreads, 0, st>>>(
+        h, hu, hv, pitch, domain_mask, rows, cols, k, scratch, max_inverse_dt_out);
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
 
 int swe_set_timing(swe_domain_t d, int32_t enable) {
     if (!d) return fail(SWE_ERR_INVALID, "null domain");

@@ -21,6 +21,8 @@ SWE_ERR_NO_DEVICE = 5
 SWE_ARITH_EXACT = 0
 SWE_ARITH_FAST = 1
 
+SWE_NOALLOC_MAX_CELLS = 16_777_216
+
 #: Every entry point ``include/swe_b200.h`` declares.
 EXPORTS = (
     "swe_domain_create",
@@ -34,6 +36,7 @@ EXPORTS = (
     "swe_last_launch_count",
     "swe_set_timing",
     "swe_last_step_time",
+    "swe_max_inverse_dt_noalloc",
     "swe_last_error",
     "swe_version",
 )
@@ -107,6 +110,8 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_last_launch_count": (ctypes.c_int64, [_vp]),
         "swe_set_timing": (ctypes.c_int, [_vp, _i32]),
         "swe_last_step_time": (ctypes.c_int, [_vp, ctypes.POINTER(_f64), ctypes.POINTER(_i64)]),
+        "swe_max_inverse_dt_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _i32, _i32, _f64,
+                                                      _f64, _f64, _f64, _vp, _vp]),
         "swe_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
         "swe_version": (ctypes.c_char_p, []),
     }

@@ -140,6 +140,29 @@ int swe_set_timing(swe_domain_t d, int32_t enable);
  * kernel of the last timed swe_run/swe_advance, and the step launches between. */
 int swe_last_step_time(swe_domain_t d, double *ms, int64_t *step_launches);
 
+/* Largest cell count swe_max_inverse_dt_noalloc accepts (a 4096 x 4096 grid). */
+#define SWE_NOALLOC_MAX_CELLS 16777216
+
+/* swe_max_inverse_dt without any memory allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc when they need
+ * a CFL step -- code running under a framework's caching allocator, where a
+ * direct cudaMalloc can fail although the framework's pool has room, and
+ * time-stepping loops that forbid allocation once running.  It needs no
+ * domain: the caller passes the state, the uint8 domain mask (rows*cols,
+ * contiguous) and the controls, and a DEVICE float that receives the maximum.
+ * Its scratch (32 KiB of per-CTA maxima plus a counter) is one fixed device
+ * array inside the library, held on every GPU that loads the library until the
+ * process exits, so grids above SWE_NOALLOC_MAX_CELLS cells are rejected with
+ * SWE_ERR_INVALID.  The first call on each device looks up that array's
+ * address; make that first call before any stream capture.  All calls share
+ * the array: calls that can overlap on the GPU (different streams, or
+ * different host threads) race and must be serialised by the caller.
+ * Arithmetic is the exact (reference-rounded) one. */
+int swe_max_inverse_dt_noalloc(const float *h, const float *hu, const float *hv, int64_t pitch,
+                               const uint8_t *domain_mask, int32_t rows, int32_t cols,
+                               double gravity, double dry_tolerance, double dx, double dy,
+                               float *max_inverse_dt_out, void *stream);
+
 /* Copy the message of the last error on this thread into buf (NUL-terminated);
  * returns the full message length. */
 int swe_last_error(char *buf, size_t n);
