@@ -55,10 +55,10 @@ BYTES_PER_CELL = 32  # h, hu, hv, bed, n^2 read (20 B) + h, hu, hv written (12 B
 def _args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--arith", choices=["exact", "fast"], default="exact")
+    ap.add_argument("--arith", choices=["exact", "fast"], default="fast")
     ap.add_argument("--rows", type=int, default=2048)
     ap.add_argument("--cols", type=int, default=2048)
     ap.add_argument("--spinup", type=int, default=200)
@@ -106,6 +106,10 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            deadline = time.time() + 3.0
+            while not self.lines and time.time() < deadline:  # sampler running before timing
+                time.sleep(0.02)
+            self.lines.clear()
         except (OSError, FileNotFoundError):
             self.proc = None
         return self

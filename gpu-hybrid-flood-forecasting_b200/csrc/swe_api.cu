@@ -18,6 +18,7 @@
 
 #include "swe_b200.h"
 #include "swe_step.cuh"
+#include "swe_step_pair.cuh"
 
 using namespace swe;
 
@@ -102,28 +103,34 @@ struct swe_domain {
     int64_t timed_steps = 0;
     int64_t launches = 0;
     int rows_per_warp_override = 0;
-    int run_vec = 2;     // vector width of the run-mode kernel (SWE_RUN_VEC=1|2|4)
+    int run_vec = 2;     // lane width of the run-mode kernel (SWE_RUN_VEC=1|2)
     bool masked = true;  // false when every cell is active (mask-free kernels)
 };
 
 namespace {
 
 // Kernel instance for (vector width, arithmetic, run mode, masked) chosen at run time.
+// V = 2 runs the paired-lane kernel; V = 1 (pitches or pointers that are not
+// 8-byte aligned) the scalar one.
 template <int V, class M, bool RUN, bool MASKED>
 struct StepK {
-    static const void* fn() { return reinterpret_cast<const void*>(&step_kernel<V, M, kThreads, RUN, MASKED>); }
+    static const void* fn() {
+        if constexpr (V == 2)
+            return reinterpret_cast<const void*>(&step_kernel_pair<M, kThreads, RUN, MASKED>);
+        else
+            return reinterpret_cast<const void*>(&step_kernel<V, M, kThreads, RUN, MASKED>);
+    }
     static void launch(int blocks, const StepLaunch& sl, cudaStream_t st) {
-        step_kernel<V, M, kThreads, RUN, MASKED><<<blocks, kThreads, 0, st>>>(sl);
+        if constexpr (V == 2)
+            step_kernel_pair<M, kThreads, RUN, MASKED><<<blocks, kThreads, 0, st>>>(sl);
+        else
+            step_kernel<V, M, kThreads, RUN, MASKED><<<blocks, kThreads, 0, st>>>(sl);
     }
 };
 
 template <class M, bool RUN, bool MASKED, class F>
 void dispatch_v(int V, F&& f) {
-    switch (V) {
-        case 4: f(StepK<4, M, RUN, MASKED>{}); break;
-        case 2: f(StepK<2, M, RUN, MASKED>{}); break;
-        default: f(StepK<1, M, RUN, MASKED>{}); break;
-    }
+    if (V == 2) f(StepK<2, M, RUN, MASKED>{}); else f(StepK<1, M, RUN, MASKED>{});
 }
 
 template <class F>
@@ -152,11 +159,12 @@ Plan make_plan(const swe_domain* d, int V, bool run) {
     const int rows = d->dd.rows, cols = d->dd.cols;
     p.nstrips = (cols + kWarp * V - 1) / (kWarp * V);
     int occ = 1;
-    dispatch(V, d->arith, run, d->masked, [&](auto k) {
+    auto occ_of = [&](auto k) {
         int n = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, decltype(k)::fn(), kThreads, 0) == cudaSuccess && n > 0)
             occ = n;
-    });
+    };
+    dispatch(V, d->arith, run, d->masked, occ_of);
     const int wpb = kThreads / kWarp;
     const int64_t warps_avail = (int64_t)occ * d->sms * wpb;
     int R = d->rows_per_warp_override;
@@ -197,7 +205,6 @@ int choose_vec(const void* const* ptrs, int n, int64_t pitch_a, int64_t pitch_b)
             if (reinterpret_cast<uintptr_t>(ptrs[i]) % bytes) return false;
         return true;
     };
-    if (pitch_a % 4 == 0 && pitch_b % 4 == 0 && aligned(16)) return 4;
     if (pitch_a % 2 == 0 && pitch_b % 2 == 0 && aligned(8)) return 2;
     return 1;
 }
@@ -213,7 +220,7 @@ int ensure_parts(swe_domain* d, int blocks) {
 
 int ensure_ping(swe_domain* d) {
     if (d->ping[0][0]) return SWE_OK;
-    d->ppitch = round_up(d->dd.cols, 32);
+    d->ppitch = round_up(d->dd.cols, 128);
     const size_t plane = sizeof(float) * (size_t)d->ppitch * (size_t)d->dd.rows;
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 3; ++f) {
@@ -517,13 +524,16 @@ int swe_domain_create(const swe_domain_desc* desc, swe_domain_t* out) {
     d->device = dev;
     d->sms = prop.multiProcessorCount;
     d->arith = q.arithmetic;
+    // Fast arithmetic runs paired lanes; exact arithmetic gains nothing from
+    // pairing (its operations stay scalar) and runs the scalar-lane kernel.
+    d->run_vec = q.arithmetic == SWE_ARITH_FAST ? 2 : 1;
     if (const char* e = std::getenv("SWE_ROWS_PER_WARP")) d->rows_per_warp_override = std::atoi(e);
     if (const char* e = std::getenv("SWE_RUN_VEC")) {
         const int v = std::atoi(e);
-        if (v == 1 || v == 2 || v == 4) d->run_vec = v;
+        if (v == 1 || v == 2) d->run_vec = v;
     }
     const int rows = q.rows, cols = q.cols;
-    const int64_t pitch = round_up(cols, 32);
+    const int64_t pitch = round_up(cols, 128);
     const size_t plane = sizeof(float) * (size_t)pitch * rows;
     const size_t n = (size_t)rows * cols;
     auto bail = [&](int code) { free_domain(d); return code; };

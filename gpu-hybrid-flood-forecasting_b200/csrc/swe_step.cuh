@@ -376,11 +376,15 @@ struct StepAccum {
 // order, so the ledger is bitwise reproducible) and advance the control block.
 template <int THREADS>
 __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts, Accum acc,
-                                bool init) {
+                                bool init, bool failed = false) {
     constexpr int W = THREADS / kWarp;
     __shared__ float s_max[W];
     __shared__ double s_sum[5][W];
     __shared__ bool s_last;
+    __shared__ int s_bad;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    if (failed) s_bad = 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     acc.maxinv = warp_max(acc.maxinv);
     acc.vol = warp_sum(acc.vol);
@@ -400,7 +404,7 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     if (threadIdx.x == 0) {
         Partial p;
         p.maxinv = s_max[0];
-        p.bad = 0;
+        p.bad = s_bad;
         p.vol = s_sum[0][0]; p.rain = s_sum[1][0]; p.outflow = s_sum[2][0];
         p.clip = s_sum[3][0]; p.mask = s_sum[4][0];
         for (int w = 1; w < W; ++w) {
@@ -419,13 +423,16 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     // Fixed-order fold of all CTA partials: thread t folds partials t, t+T, ...
     Accum a;
     a.zero();
+    int bad = 0;
     const volatile Partial* vp = parts;
     for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS) {
+        bad |= vp[b].bad;
         a.maxinv = nan_max(a.maxinv, vp[b].maxinv);
         a.vol += vp[b].vol; a.rain += vp[b].rain; a.outflow += vp[b].outflow;
         a.clip += vp[b].clip; a.mask += vp[b].mask;
     }
     __syncthreads();
+    bad = __syncthreads_or(bad);
     a.maxinv = warp_max(a.maxinv);
     a.vol = warp_sum(a.vol); a.rain = warp_sum(a.rain); a.outflow = warp_sum(a.outflow);
     a.clip = warp_sum(a.clip); a.mask = warp_sum(a.mask);
@@ -468,6 +475,11 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     c.maxinv = mx;
     c.counter = 0;
     plan_next(d, c);
+    if (bad) {  // a bounded device wait ran out: stop the run and report it
+        c.status = 6;  // SWE_ERR_TIMEOUT
+        c.done = 1;
+        c.snap = -1;
+    }
     *ctl = c;
     __threadfence();
 }
@@ -487,9 +499,12 @@ struct StepLaunch {
 };
 
 // Resident CTAs per SM the register budget is capped for (V=2: 128 registers).
+#ifndef SWE_MINBLOCKS_V2
+#define SWE_MINBLOCKS_V2 4
+#endif
 template <int V>
 struct MinBlocks {
-    static constexpr int value = V == 1 ? 4 : (V == 2 ? 4 : 2);
+    static constexpr int value = V == 1 ? 4 : (V == 2 ? SWE_MINBLOCKS_V2 : 2);
 };
 
 template <int V, class M, int THREADS, bool RUN, bool MASKED>
