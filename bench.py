@@ -64,6 +64,9 @@ def _args():
     ap.add_argument("--spinup", type=int, default=200)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-members", type=int, default=64)
+    ap.add_argument("--ensemble-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -169,6 +172,59 @@ def _cpu_port_time(w, depth, steps: int, threads: int):
     return el / steps, w.bed.size
 
 
+def _ensemble(args, dev, world: int):
+    """Batched 64-member ensemble vs the same members run one by one (plain path)."""
+    import torch
+
+    from hybrid_flood_b200.ensemble import B200Ensemble
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver, ledger_error
+    from hybrid_flood_b200.workloads import as_member, ensemble_members, street_depth
+
+    ws = ensemble_members(args.ensemble_members)
+    members = [as_member(w) for w in ws]
+    depths = [street_depth(w) for w in ws]
+    ens = B200Ensemble(members, arithmetic=args.arith, device=dev)
+    states = ens.initial_states(depths)
+    ens.advance_(states, 50)  # spin-up
+    tune_states = [type(s)(*(t.clone() for t in s)) for s in states]
+    best = ens.autotune(tune_states, candidates=(8, 16, 32, 64), steps=10, cache=None)
+    del tune_states
+    ens.advance_(states, 10)  # warm-up (graph capture)
+    ens.set_timing(True)
+    res = ens.advance_(states, args.ensemble_steps)
+    ms, n = ens.last_step_time()
+    cells = ens.cells
+    value = cells * n / (ms / 1e3)
+    worst_ledger = max(ledger_error(r[2]) for r in res)
+    # Plain path, member after member, same steps (each member its own solver).
+    solvers = [B200ShallowWaterSolver(m["bed"], m["manning_n"], m["domain_mask"],
+                                      **{k: v for k, v in m.items() if k not in ("bed", "manning_n", "domain_mask")},
+                                      arithmetic=args.arith, device=dev) for m in members]
+    plain_states = [s.initial_state(depth_m=d) for s, d in zip(solvers, depths)]
+    for s, st in zip(solvers, plain_states):
+        s.advance_(st, 10)
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s, st in zip(solvers, plain_states):
+        s.advance_(st, args.ensemble_steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    plain_ms = e0.elapsed_time(e1)
+    plain_value = cells * args.ensemble_steps / (plain_ms / 1e3)
+    peak, kind = _peaks()
+    return {
+        "value": value * world, "unit": "cell-updates/s", "members": len(members), "cells": cells,
+        "steps": n, "ms_per_step": ms / n, "rows_per_warp": best,
+        "roofline_frac": BYTES_PER_CELL * value / 1e9 / peak, "peak_kind": kind,
+        "plain_sequential_value": plain_value * world, "speedup_vs_plain_sequential": value / plain_value,
+        "ledger_rel_error_max": worst_ledger, "gpu_launches": ens.last_launch_count(),
+        "workload": f"{len(members)} urban members from {{256^2, 512^2, 1024^2, 768x1536}}, dx=1m, "
+                    "rain x LogNormal(0.4), n x U(0.8,1.2), seeds 1000+m",
+    }
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
@@ -270,6 +326,9 @@ def run_b200(args, rank: int, world: int):
                "call": "B200ShallowWaterSolver.run(host NumPy state, [0, window]) + final state to host",
                "steps_per_call": steps_e2e / reps, "wall_s": wall}
 
+    ens = None
+    if not args.no_ensemble:
+        ens = _ensemble(args, dev, world)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -297,6 +356,8 @@ def run_b200(args, rank: int, world: int):
     }
     if e2e:
         line["e2e"] = e2e
+    if ens:
+        line["ensemble"] = ens
     if not args.no_cpu_baseline:
         from oracle import cport
 

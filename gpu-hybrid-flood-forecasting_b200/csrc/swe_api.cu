@@ -243,15 +243,16 @@ int copy_plane(float* dst, int64_t dpitch, const float* src, int64_t spitch, int
     return SWE_OK;
 }
 
-// Shared run driver for swe_run and swe_advance.
-int run_driver(swe_domain* d, StateView init, const float* times_host, int n_times,
-               double t_start, int n_out, int max_steps, float* out_h, float* out_hu,
-               float* out_hv, swe_run_result* res, cudaStream_t st, int* final_buf) {
+// Load the initial state into ping buffer 0, upload the output times, write
+// snapshot 0, reset the run control and launch the reduction that sets the
+// clock, the first CFL dt and volume0.  Shared by swe_run, swe_advance and the
+// ensemble.
+int begin_run(swe_domain* d, StateView init, const float* times_host, int n_times, double t_start,
+              int n_out, int max_steps, float* out_h, float* out_hu, float* out_hv, cudaStream_t st) {
     const int rows = d->dd.rows, cols = d->dd.cols;
     int rc = ensure_ping(d);
     if (rc) return rc;
-    const Plan pl = make_plan(d, d->run_vec, true);
-    rc = ensure_parts(d, std::max(pl.blocks, reduce_blocks(d)));
+    rc = ensure_parts(d, reduce_blocks(d));
     if (rc) return rc;
     for (int f = 0; f < 3; ++f) {
         const float* src = f == 0 ? init.h : (f == 1 ? init.hu : init.hv);
@@ -290,6 +291,20 @@ int run_driver(swe_domain* d, StateView init, const float* times_host, int n_tim
     StateView v0{d->ping[0][0], d->ping[0][1], d->ping[0][2], d->ppitch};
     launch_reduce(d, v0, d->ctl, st);
     SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
+// Shared run driver for swe_run and swe_advance.
+int run_driver(swe_domain* d, StateView init, const float* times_host, int n_times,
+               double t_start, int n_out, int max_steps, float* out_h, float* out_hu,
+               float* out_hv, swe_run_result* res, cudaStream_t st, int* final_buf) {
+    int rc = ensure_ping(d);
+    if (rc) return rc;
+    const Plan pl = make_plan(d, d->run_vec, true);
+    rc = ensure_parts(d, std::max(pl.blocks, reduce_blocks(d)));
+    if (rc) return rc;
+    rc = begin_run(d, init, times_host, n_times, t_start, n_out, max_steps, out_h, out_hu, out_hv, st);
+    if (rc) return rc;
     int64_t launched = 0;
     d->launches = 1;
     d->timed_valid = false;
@@ -381,6 +396,144 @@ __global__ void pack_static_kernel(const float* bed, const float* man, const uin
         if (!mask[j]) *any_inactive = 1;
         if (mult_o) mult_o[i] = mult[j];
     }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Batched ensemble (swe_ensemble_*)
+// ---------------------------------------------------------------------------
+struct swe_ensemble {
+    std::vector<swe_domain*> doms;
+    int arith = SWE_ARITH_FAST;
+    bool masked = false;
+    int rows_per_warp = 16;
+    int sms = 148;
+    MemberDev* members_dev = nullptr;
+    int members_cap = 0;
+    int2* items_dev = nullptr;
+    int items_cap = 0;
+    int n_items = 0;
+    int grid = 1;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_k = 0;
+    cudaEvent_t time_ev[2] = {nullptr, nullptr};
+    bool timing = false;
+    bool timed_valid = false;
+    int64_t timed_steps = 0;
+    int64_t launches = 0;
+};
+
+namespace {
+
+template <class M, bool MASKED>
+void ens_launch_t(const swe_ensemble* e, int parity, cudaStream_t st) {
+    ensemble_step_kernel<M, kThreads, MASKED><<<e->grid, kThreads, 0, st>>>(e->members_dev, e->items_dev,
+                                                                            e->n_items, parity);
+}
+
+void ens_launch(const swe_ensemble* e, int parity, cudaStream_t st) {
+    if (e->arith == SWE_ARITH_FAST) {
+        if (e->masked) ens_launch_t<FastMath, true>(e, parity, st); else ens_launch_t<FastMath, false>(e, parity, st);
+    } else {
+        if (e->masked) ens_launch_t<ExactMath, true>(e, parity, st); else ens_launch_t<ExactMath, false>(e, parity, st);
+    }
+}
+
+int ens_occupancy(const swe_ensemble* e) {
+    const void* fn = nullptr;
+    if (e->arith == SWE_ARITH_FAST)
+        fn = e->masked ? reinterpret_cast<const void*>(&ensemble_step_kernel<FastMath, kThreads, true>)
+                       : reinterpret_cast<const void*>(&ensemble_step_kernel<FastMath, kThreads, false>);
+    else
+        fn = e->masked ? reinterpret_cast<const void*>(&ensemble_step_kernel<ExactMath, kThreads, true>)
+                       : reinterpret_cast<const void*>(&ensemble_step_kernel<ExactMath, kThreads, false>);
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kThreads, 0) != cudaSuccess || n < 1) n = 1;
+    return n;
+}
+
+// Member table and work list for the current rows-per-warp.
+int ens_rebuild(swe_ensemble* e) {
+    const int wpb = kThreads / kWarp;
+    const int R = e->rows_per_warp;
+    std::vector<MemberDev> md(e->doms.size());
+    std::vector<int2> items;
+    for (size_t m = 0; m < e->doms.size(); ++m) {
+        swe_domain* d = e->doms[m];
+        int rc = ensure_ping(d);
+        if (rc) return rc;
+        const int nstrips = (d->dd.cols + 2 * kWarp - 1) / (2 * kWarp);
+        const int chunks = (d->dd.rows + R - 1) / R;
+        const int ncta = (int)(((int64_t)chunks * nstrips + wpb - 1) / wpb);
+        rc = ensure_parts(d, std::max(ncta, reduce_blocks(d)));
+        if (rc) return rc;
+        MemberDev& x = md[m];
+        x.d = d->dd;
+        for (int b = 0; b < 2; ++b)
+            for (int f = 0; f < 3; ++f) x.buf[b][f] = d->ping[b][f];
+        x.pitch = d->ppitch;
+        x.ctl = d->ctl;
+        x.parts = d->parts;
+        x.nstrips = nstrips;
+        x.rows_per_warp = R;
+        x.ncta = ncta;
+        for (int c = 0; c < ncta; ++c) items.push_back(make_int2((int)m, c));
+    }
+    if ((int)md.size() > e->members_cap) {
+        cudaFree(e->members_dev);
+        e->members_dev = nullptr;
+        SWE_CK(cudaMalloc(&e->members_dev, sizeof(MemberDev) * md.size()));
+        e->members_cap = (int)md.size();
+    }
+    if ((int)items.size() > e->items_cap) {
+        cudaFree(e->items_dev);
+        e->items_dev = nullptr;
+        SWE_CK(cudaMalloc(&e->items_dev, sizeof(int2) * items.size()));
+        e->items_cap = (int)items.size();
+    }
+    SWE_CK(cudaMemcpy(e->members_dev, md.data(), sizeof(MemberDev) * md.size(), cudaMemcpyHostToDevice));
+    SWE_CK(cudaMemcpy(e->items_dev, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice));
+    e->n_items = (int)items.size();
+    e->grid = std::max(1, std::min(e->n_items, ens_occupancy(e) * e->sms));
+    if (e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+        e->graph_k = 0;
+    }
+    return SWE_OK;
+}
+
+// CUDA graph of K consecutive ensemble steps (parity alternating, K even).
+int ens_graph(swe_ensemble* e, int K) {
+    if (e->graph && e->graph_k == K) return SWE_OK;
+    if (e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    if (!e->cap_stream) SWE_CK(cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking));
+    SWE_CK(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < K; ++k) ens_launch(e, k & 1, e->cap_stream);
+    cudaGraph_t g = nullptr;
+    SWE_CK(cudaStreamEndCapture(e->cap_stream, &g));
+    const cudaError_t err = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (err != cudaSuccess) return fail(SWE_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(err));
+    e->graph_k = K;
+    return SWE_OK;
+}
+
+void free_ensemble(swe_ensemble* e) {
+    if (!e) return;
+    for (auto* d : e->doms) free_domain(d);
+    cudaFree(e->members_dev);
+    cudaFree(e->items_dev);
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
+    for (int i = 0; i < 2; ++i)
+        if (e->time_ev[i]) cudaEventDestroy(e->time_ev[i]);
+    delete e;
 }
 
 }  // namespace
@@ -766,6 +919,140 @@ int swe_advance(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, i
 }
 
 int64_t swe_last_launch_count(swe_domain_t d) { return d ? d->launches : -1; }
+
+int swe_ensemble_create(const swe_domain_desc* descs, int32_t n_members, swe_ensemble_t* out) {
+    if (!descs || !out || n_members < 1) return fail(SWE_ERR_INVALID, "need at least one member descriptor");
+    *out = nullptr;
+    for (int m = 1; m < n_members; ++m)
+        if (descs[m].arithmetic != descs[0].arithmetic)
+            return fail(SWE_ERR_INVALID, "all ensemble members must use the same arithmetic");
+    swe_ensemble* e = new swe_ensemble();
+    e->arith = descs[0].arithmetic;
+    if (const char* v = std::getenv("SWE_ENSEMBLE_ROWS")) {
+        const int r = std::atoi(v);
+        if (r > 0) e->rows_per_warp = r;
+    }
+    for (int m = 0; m < n_members; ++m) {
+        swe_domain_t d = nullptr;
+        const int rc = swe_domain_create(&descs[m], &d);
+        if (rc) {
+            free_ensemble(e);
+            return rc;
+        }
+        e->doms.push_back(d);
+        e->masked = e->masked || d->masked;
+        e->sms = d->sms;
+    }
+    const int rc = ens_rebuild(e);
+    if (rc) {
+        free_ensemble(e);
+        return rc;
+    }
+    *out = e;
+    return SWE_OK;
+}
+
+int swe_ensemble_destroy(swe_ensemble_t e) {
+    if (!e) return SWE_OK;
+    cudaDeviceSynchronize();
+    free_ensemble(e);
+    return SWE_OK;
+}
+
+int swe_ensemble_size(swe_ensemble_t e) { return e ? (int)e->doms.size() : -1; }
+
+int swe_ensemble_set_rows_per_warp(swe_ensemble_t e, int32_t rows_per_warp) {
+    if (!e || rows_per_warp < 1) return fail(SWE_ERR_INVALID, "rows_per_warp must be >= 1");
+    cudaDeviceSynchronize();
+    e->rows_per_warp = rows_per_warp;
+    return ens_rebuild(e);
+}
+
+int swe_ensemble_advance(swe_ensemble_t e, float* const* h, float* const* hu, float* const* hv,
+                         const int64_t* pitch, int32_t n_steps, const double* start_s,
+                         swe_run_result* results, void* stream) {
+    if (!e || !h || !hu || !hv || !pitch || !results) return fail(SWE_ERR_INVALID, "null argument");
+    if (n_steps < 0) return fail(SWE_ERR_INVALID, "n_steps must be >= 0");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int n = (int)e->doms.size();
+    for (int m = 0; m < n; ++m) {
+        swe_domain* d = e->doms[m];
+        int rc = check_state_ptrs(h[m], hu[m], hv[m], pitch[m], d->dd.cols);
+        if (rc) return rc;
+        const double t0 = start_s ? start_s[m] : 0.0;
+        const float times[2] = {(float)t0, INFINITY};
+        rc = begin_run(d, StateView{h[m], hu[m], hv[m], pitch[m]}, times, 2, t0, 2, n_steps, nullptr,
+                       nullptr, nullptr, st);
+        if (rc) return rc;
+    }
+    const int K = 50;
+    e->timed_valid = false;
+    if (e->timing) {
+        if (!e->time_ev[0]) {
+            SWE_CK(cudaEventCreate(&e->time_ev[0]));
+            SWE_CK(cudaEventCreate(&e->time_ev[1]));
+        }
+        SWE_CK(cudaEventRecord(e->time_ev[0], st));
+    }
+    int64_t done_steps = 0;
+    if (n_steps >= K) {
+        int rc = ens_graph(e, K);
+        if (rc) return rc;
+        for (; done_steps + K <= n_steps; done_steps += K) SWE_CK(cudaGraphLaunch(e->graph, st));
+    }
+    for (; done_steps < n_steps; ++done_steps) ens_launch(e, (int)(done_steps & 1), st);
+    SWE_CK(cudaGetLastError());
+    e->launches = n + n_steps;
+    if (e->timing) {
+        SWE_CK(cudaEventRecord(e->time_ev[1], st));
+        e->timed_steps = n_steps;
+        e->timed_valid = true;
+    }
+    SWE_CK(cudaStreamSynchronize(st));
+    int status = SWE_OK;
+    for (int m = 0; m < n; ++m) {
+        swe_domain* d = e->doms[m];
+        SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
+        const Control& c = d->ctl_host[0];
+        swe_run_result& r = results[m];
+        r.final_time_s = c.t;
+        r.outputs_written = c.idx;
+        r.steps_used = c.steps;
+        r.status = c.status;
+        r.reserved = 0;
+        for (int i = 0; i < 6; ++i) r.ledger[i] = c.ledger[i];
+        if (c.status) status = c.status;
+        float* outs[3] = {h[m], hu[m], hv[m]};
+        const int fb = c.steps & 1;
+        for (int f = 0; f < 3; ++f) {
+            const int rc = copy_plane(outs[f], pitch[m], d->ping[fb][f], d->ppitch, d->dd.rows, d->dd.cols, st);
+            if (rc) return rc;
+        }
+    }
+    SWE_CK(cudaStreamSynchronize(st));
+    if (status == SWE_ERR_NONFINITE) return fail(SWE_ERR_NONFINITE, "non-finite values reached a member's CFL reduction");
+    if (status) return fail(status, "an ensemble member stopped with an error status");
+    return SWE_OK;
+}
+
+int swe_ensemble_set_timing(swe_ensemble_t e, int32_t enable) {
+    if (!e) return fail(SWE_ERR_INVALID, "null ensemble");
+    e->timing = enable != 0;
+    return SWE_OK;
+}
+
+int swe_ensemble_last_step_time(swe_ensemble_t e, double* ms, int64_t* steps) {
+    if (!e || !ms || !steps) return fail(SWE_ERR_INVALID, "null argument");
+    if (!e->timed_valid) return fail(SWE_ERR_INVALID, "no timed advance recorded (call swe_ensemble_set_timing first)");
+    float f = 0.f;
+    SWE_CK(cudaEventElapsedTime(&f, e->time_ev[0], e->time_ev[1]));
+    *ms = (double)f;
+    *steps = e->timed_steps;
+    return SWE_OK;
+}
+
+int64_t swe_ensemble_last_launch_count(swe_ensemble_t e) { return e ? e->launches : -1; }
+
 
 int swe_max_inverse_dt_noalloc(const float* h, const float* hu, const float* hv, int64_t pitch,
                                const uint8_t* domain_mask, int32_t rows, int32_t cols,

@@ -355,19 +355,17 @@ struct Accum {
 // Per-thread accumulators of the step kernel.  Without a rain-multiplier plane
 // every active cell receives the same float32 increment, so the rain term is
 // kept as a cell count and multiplied out once per thread.
-// Stored volume is summed in float64 per cell; the other terms (edge fluxes,
-// positivity-clip and masked-cell corrections) are a few small values per
-// thread and are summed in float32 before the float64 reduction across threads.
+// Every ledger term is summed in float64 from the first cell on (a float32
+// partial over a warp's rows already costs ~1e-6 of the ledger); without a
+// rain-multiplier plane the rain term is an exact count of active cells.
 struct StepAccum {
     float maxinv;
     unsigned rain_cells;
-    double vol;
-    float rain, outflow, clip, mask;
+    double vol, rain, outflow, clip, mask;
     __device__ void zero() {
         maxinv = 0.f;
         rain_cells = 0u;
-        vol = 0.0;
-        rain = outflow = clip = mask = 0.f;
+        vol = rain = outflow = clip = mask = 0.0;
     }
 };
 
@@ -376,7 +374,13 @@ struct StepAccum {
 // order, so the ledger is bitwise reproducible) and advance the control block.
 template <int THREADS>
 __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts, Accum acc,
-                                bool init, bool failed = false) {
+                                bool init, bool failed = false, int part = -1, int nparts = -1) {
+    // One partial per CTA of this domain: by default the launch's CTAs; the
+    // ensemble kernel passes the CTA's slot within its member instead.
+    if (part < 0) {
+        part = blockIdx.x;
+        nparts = gridDim.x;
+    }
     constexpr int W = THREADS / kWarp;
     __shared__ float s_max[W];
     __shared__ double s_sum[5][W];
@@ -412,10 +416,10 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
             p.vol += s_sum[0][w]; p.rain += s_sum[1][w]; p.outflow += s_sum[2][w];
             p.clip += s_sum[3][w]; p.mask += s_sum[4][w];
         }
-        parts[blockIdx.x] = p;
+        parts[part] = p;
         __threadfence();
         const unsigned ticket = atomicAdd(&ctl->counter, 1u);
-        s_last = (ticket == gridDim.x - 1);
+        s_last = (ticket == (unsigned)nparts - 1);
     }
     __syncthreads();
     if (!s_last) return;
@@ -425,7 +429,7 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     a.zero();
     int bad = 0;
     const volatile Partial* vp = parts;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS) {
+    for (int b = threadIdx.x; b < nparts; b += THREADS) {
         bad |= vp[b].bad;
         a.maxinv = nan_max(a.maxinv, vp[b].maxinv);
         a.vol += vp[b].vol; a.rain += vp[b].rain; a.outflow += vp[b].outflow;
@@ -555,7 +559,7 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
             yT0[i] = f.f0;
             yT1[i] = f.f1;
             yT2[i] = M::add(f.f2, f.corr_hi);
-            if (run && r0 == 0 && c0 + i < d.cols) acc.outflow -= (float)(dtd * (double)f.f0 * d.dx);
+            if (run && r0 == 0 && c0 + i < d.cols) acc.outflow -= dtd * (double)f.f0 * d.dx;
         }
         load_cells<V>(d, p.in, r0 + 1, c0, C);
 #pragma unroll
@@ -579,7 +583,7 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
                 s_left[wib][0][lane] = f.f0;
                 s_left[wib][1][lane] = M::add(f.f1, f.corr_hi);
                 s_left[wib][2][lane] = f.f2;
-                if (run && x0w == 0 && r + lane < r1) acc.outflow -= (float)(dtd * (double)f.f0 * d.dy);
+                if (run && x0w == 0 && r + lane < r1) acc.outflow -= dtd * (double)f.f0 * d.dy;
                 s_right[wib][0][lane] = R[0].h;
                 s_right[wib][1][lane] = R[0].hu;
                 s_right[wib][2][lane] = R[0].hv;
@@ -602,7 +606,7 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
                 yN0[i] = f.f0;
                 yN1[i] = f.f1;
                 yN2[i] = M::add(f.f2, f.corr_hi);
-                if (run && r == d.rows - 1 && c0 + i < d.cols) acc.outflow += (float)(dtd * (double)f.f0 * d.dx);
+                if (run && r == d.rows - 1 && c0 + i < d.cols) acc.outflow += dtd * (double)f.f0 * d.dx;
             }
             // x-faces of row r: right neighbour of each lane's last cell.
             Cell rn;
@@ -638,7 +642,7 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
                     xr1[0] = __shfl_up_sync(0xffffffffu, h1, 1);
                     xr2[0] = __shfl_up_sync(0xffffffffu, h2, 1);
                 }
-                if (run && c0 + i == d.cols - 1) acc.outflow += (float)(dtd * (double)f.f0 * d.dy);
+                if (run && c0 + i == d.cols - 1) acc.outflow += dtd * (double)f.f0 * d.dy;
             }
             {
                 const float l0 = s_left[wib][0][j], l1 = s_left[wib][1][j], l2 = s_left[wib][2][j];
@@ -692,9 +696,9 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
                     const float inv = M::add(M::div(M::add(fabsf(u), w), k.dx), M::div(M::add(fabsf(v), w), k.dy));
                     acc.maxinv = nan_max(acc.maxinv, act ? inv : 0.0f);
                     acc.vol += (double)ho[i];
-                    if (d.mult != nullptr) acc.rain += rain; else acc.rain_cells += act ? 1u : 0u;
-                    if (upd[0] < 0.0f) acc.clip -= upd[0];
-                    if (MASKED && !act) acc.mask += h;
+                    if (d.mult != nullptr) acc.rain += (double)rain; else acc.rain_cells += act ? 1u : 0u;
+                    if (upd[0] < 0.0f) acc.clip -= (double)upd[0];
+                    if (MASKED && !act) acc.mask += (double)h;
                 }
             }
             // Store row r.
@@ -758,10 +762,10 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
         Accum a;
         a.maxinv = acc.maxinv;
         a.vol = acc.vol;
-        a.rain = (double)acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
-        a.outflow = (double)acc.outflow;
-        a.clip = (double)acc.clip;
-        a.mask = (double)acc.mask;
+        a.rain = acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
+        a.outflow = acc.outflow;
+        a.clip = acc.clip;
+        a.mask = acc.mask;
         finish_run_step<THREADS>(d, p.ctl, p.parts, a, false);
     }
 }

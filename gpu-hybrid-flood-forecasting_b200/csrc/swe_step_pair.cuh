@@ -63,55 +63,42 @@ __device__ __forceinline__ void cp_async_wait() {
 #define SWE_PAIR_MINBLOCKS 4
 #endif
 
-template <class M, int THREADS, bool RUN, bool MASKED>
-__global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(const StepLaunch p) {
-    constexpr int NW = THREADS / kWarp;
+// Warp-private shared memory of the march: strip edges of the current 32-row
+// batch and the cp.async row ring.
+struct WarpSmem {
+    float left[3][kWarp];      // hi side of the strip's left x-face, per batch row
+    float right[7][kWarp];     // the cell right of the strip, per batch row
+    float2 ring[kRing][5][kWarp];  // [slot][field][lane]
+};
+
+// One warp marches rows [r0, r1) of the 64-column strip starting at x0w: every
+// face once, cells updated, row r written to `out` (and to snapshot `snap` of
+// `ctl` in run mode); CFL maximum and ledger terms accumulate into `acc`.
+template <class M, bool RUN, bool MASKED>
+__device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& in,
+                                           const StateOut& out, const StepScalars& s, int snap,
+                                           double dtd, const Control* ctl, int r0, int r1,
+                                           int x0w, WarpSmem& sm, StepAccum& acc) {
     constexpr int kBatch = kWarp;
     constexpr int V = 2;
     using A = P<M>;
-    __shared__ float s_left[NW][3][kBatch];
-    __shared__ float s_right[NW][7][kBatch];
-    __shared__ float2 s_ring[NW][kRing][5][kWarp];  // [warp][slot][field][lane]
-
-    const DomainDev& d = p.d;
     const Consts& k = d.k;
     const KPair kp = make_kpair(k);
     const KScalar ks = make_kscalar(k);
-    StepScalars s = p.s;
-    int snap = -1;
-    double dtd = 0.0;
-    if constexpr (RUN) {
-        const Control* c = p.ctl;
-        if (*((volatile const int*)&c->done)) return;  // uniform early exit of the whole grid
-        s = c->s;
-        snap = c->snap;
-        dtd = c->dt;
-    }
     const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    const int gw = blockIdx.x * NW + wib;
-    const int strip = gw % p.nstrips;
-    const int chunk = gw / p.nstrips;
-    const int r0 = chunk * p.rows_per_warp;
-    const int r1 = min(r0 + p.rows_per_warp, d.rows);
-    const int x0w = strip * kWarp * V;
     const int c0 = x0w + lane * V;
     const B2 valid{c0 < d.cols, c0 + 1 < d.cols};
     const int right_edge = d.cols - 1 - c0;  // 0 or 1 when this lane holds the last column
-    // Step constants as pairs.
     const float2 dt2 = splat(s.dt), dtr2 = splat(s.dt_rain), dtg2 = splat(s.dt_g);
     const float2 dx2 = splat(k.dx), dy2 = splat(k.dy);
     const float rdx = 1.0f / k.dx, rdy = 1.0f / k.dy;
     const float2 ndtdx2 = splat(-s.dt * rdx), ndtdy2 = splat(-s.dt * rdy);
     const float2 rdx2 = splat(rdx), rdy2 = splat(rdy);
     const float2 nexpo2 = splat(-k.expo);
-    StepAccum acc;
-    acc.zero();
-
-    if (r0 < d.rows) {
+    {
         const int nq = r1 - r0 + 2;  // rows r0-1 .. r1 pass through the ring
-        const float* planes[5] = {p.in.h, p.in.hu, p.in.hv, d.bed, d.nm};
-        const int64_t pitches[5] = {p.in.pitch, p.in.pitch, p.in.pitch, d.spitch, d.spitch};
+        const float* planes[5] = {in.h, in.hu, in.hv, d.bed, d.nm};
+        const int64_t pitches[5] = {in.pitch, in.pitch, in.pitch, d.spitch, d.spitch};
         const bool edge_strip = x0w + kWarp * V > d.cols;
         // Start the copies of ring row qi (row r0-1+qi, clamped to the grid); one group per row.
         auto issue = [&](int qi) {
@@ -122,8 +109,8 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
 #pragma unroll
                 for (int f = 0; f < 5; ++f) {
                     const float* src = planes[f] + (int64_t)rr * pitches[f] + c0;
-                    if (c0 + 1 < d.cols) cp_async_8(&s_ring[wib][st][f][lane], src);
-                    else if (c0 < d.cols) cp_async_4(&s_ring[wib][st][f][lane], src);
+                    if (c0 + 1 < d.cols) cp_async_8(&sm.ring[st][f][lane], src);
+                    else if (c0 < d.cols) cp_async_4(&sm.ring[st][f][lane], src);
                 }
             }
             cp_async_commit();
@@ -135,11 +122,11 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
             const int q = r0 - 1 + qi;
             float2 fv[5];
 #pragma unroll
-            for (int f = 0; f < 5; ++f) fv[f] = s_ring[wib][st][f][lane];
+            for (int f = 0; f < 5; ++f) fv[f] = sm.ring[st][f][lane];
             if (edge_strip) {
                 __syncwarp();  // the last column may sit in another lane's slot
                 const int last = d.cols - 1 - x0w;
-                const float* lastp = reinterpret_cast<const float*>(&s_ring[wib][st][0][0]);
+                const float* lastp = reinterpret_cast<const float*>(&sm.ring[st][0][0]);
                 float g[5];
 #pragma unroll
                 for (int f = 0; f < 5; ++f) g[f] = lastp[f * 2 * kWarp + last];
@@ -176,8 +163,8 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
             yT1 = f.f1;
             yT2 = A::add(f.f2, f.corr_hi);
             if (RUN && r0 == 0) {
-                if (valid.x) acc.outflow -= (float)(dtd * (double)f.f0.x * d.dx);
-                if (valid.y) acc.outflow -= (float)(dtd * (double)f.f0.y * d.dx);
+                if (valid.x) acc.outflow -= dtd * (double)f.f0.x * d.dx;
+                if (valid.y) acc.outflow -= dtd * (double)f.f0.y * d.dx;
             }
         }
         consume(2, Ab);  // row r0+1
@@ -189,9 +176,9 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
                 __syncwarp();
                 const int rr = min(r + lane, d.rows - 1);
                 Cell L[1], E[1], R[1];
-                load_cells<1>(d, p.in, rr, x0w - 1, L);
-                load_cells<1>(d, p.in, rr, x0w, E);
-                load_cells<1>(d, p.in, rr, x0w + kWarp * V, R);
+                load_cells<1>(d, in, rr, x0w - 1, L);
+                load_cells<1>(d, in, rr, x0w, E);
+                load_cells<1>(d, in, rr, x0w + kWarp * V, R);
                 CellT<float> l{L[0].h, L[0].hu, L[0].hv, L[0].z, L[0].nm, 0.f, 0.f};
                 CellT<float> e{E[0].h, E[0].hu, E[0].hv, E[0].z, E[0].nm, 0.f, 0.f};
                 CellT<float> q{R[0].h, R[0].hu, R[0].hv, R[0].z, R[0].nm, 0.f, 0.f};
@@ -199,17 +186,17 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
                 set_vel_t<M>(e, ks);
                 set_vel_t<M>(q, ks);
                 const FaceT<float> f = face_t<1, M, MASKED>(l, e, ks);
-                s_left[wib][0][lane] = f.f0;
-                s_left[wib][1][lane] = A::add(f.f1, f.corr_hi);
-                s_left[wib][2][lane] = f.f2;
-                if (RUN && x0w == 0 && r + lane < r1) acc.outflow -= (float)(dtd * (double)f.f0 * d.dy);
-                s_right[wib][0][lane] = q.h;
-                s_right[wib][1][lane] = q.hu;
-                s_right[wib][2][lane] = q.hv;
-                s_right[wib][3][lane] = q.z;
-                s_right[wib][4][lane] = q.nm;
-                s_right[wib][5][lane] = q.u;
-                s_right[wib][6][lane] = q.v;
+                sm.left[0][lane] = f.f0;
+                sm.left[1][lane] = A::add(f.f1, f.corr_hi);
+                sm.left[2][lane] = f.f2;
+                if (RUN && x0w == 0 && r + lane < r1) acc.outflow -= dtd * (double)f.f0 * d.dy;
+                sm.right[0][lane] = q.h;
+                sm.right[1][lane] = q.hu;
+                sm.right[2][lane] = q.hv;
+                sm.right[3][lane] = q.z;
+                sm.right[4][lane] = q.nm;
+                sm.right[5][lane] = q.u;
+                sm.right[6][lane] = q.v;
                 __syncwarp();
             }
 
@@ -218,8 +205,8 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
             const float2 yB0 = fy.f0, yB1 = fy.f1, yB2 = A::add(fy.f2, fy.corr_lo);
             const float2 yN2 = A::add(fy.f2, fy.corr_hi);
             if (RUN && r == d.rows - 1) {
-                if (valid.x) acc.outflow += (float)(dtd * (double)fy.f0.x * d.dx);
-                if (valid.y) acc.outflow += (float)(dtd * (double)fy.f0.y * d.dx);
+                if (valid.x) acc.outflow += dtd * (double)fy.f0.x * d.dx;
+                if (valid.y) acc.outflow += dtd * (double)fy.f0.y * d.dx;
             }
 
             // x-faces: (cell 0 | cell 1) and (cell 1 | first cell of the next lane).
@@ -231,9 +218,9 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
             float ru = __shfl_down_sync(0xffffffffu, cur.u.x, 1);
             float rv = __shfl_down_sync(0xffffffffu, cur.v.x, 1);
             {
-                const float e0 = s_right[wib][0][j], e1 = s_right[wib][1][j], e2 = s_right[wib][2][j];
-                const float e3 = s_right[wib][3][j], e4 = s_right[wib][4][j], e5 = s_right[wib][5][j];
-                const float e6 = s_right[wib][6][j];
+                const float e0 = sm.right[0][j], e1 = sm.right[1][j], e2 = sm.right[2][j];
+                const float e3 = sm.right[3][j], e4 = sm.right[4][j], e5 = sm.right[5][j];
+                const float e6 = sm.right[6][j];
                 if (lane == 31) {
                     rh = e0; rhu = e1; rhv = e2; rz = e3; rnm = e4; ru = e5; rv = e6;
                 }
@@ -253,14 +240,14 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
             float up1 = __shfl_up_sync(0xffffffffu, xh1.y, 1);
             float up2 = __shfl_up_sync(0xffffffffu, fx.f2.y, 1);
             {
-                const float l0 = s_left[wib][0][j], l1 = s_left[wib][1][j], l2 = s_left[wib][2][j];
+                const float l0 = sm.left[0][j], l1 = sm.left[1][j], l2 = sm.left[2][j];
                 if (lane == 0) {
                     up0 = l0; up1 = l1; up2 = l2;
                 }
             }
             const float2 xr0 = f2(up0, fx.f0.x), xr1 = f2(up1, xh1.x), xr2 = f2(up2, fx.f2.x);
             if (RUN && (right_edge == 0 || right_edge == 1))
-                acc.outflow += (float)(dtd * (double)(right_edge == 0 ? fx.f0.x : fx.f0.y) * d.dy);
+                acc.outflow += dtd * (double)(right_edge == 0 ? fx.f0.x : fx.f0.y) * d.dy;
 
             // Cell updates of both columns.
             const auto act = MASKED ? act_of(cur.nm) : all_true<float2>();
@@ -323,29 +310,29 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
                 acc.maxinv = nan_max(acc.maxinv, use.y ? inv.y : 0.0f);
                 acc.vol += (double)(valid.x ? ho.x : 0.0f) + (double)(valid.y ? ho.y : 0.0f);
                 if (d.mult != nullptr) {
-                    acc.rain += (valid.x ? rain.x : 0.0f) + (valid.y ? rain.y : 0.0f);
+                    acc.rain += (double)(valid.x ? rain.x : 0.0f) + (double)(valid.y ? rain.y : 0.0f);
                 } else {
                     acc.rain_cells += (use.x ? 1u : 0u) + (use.y ? 1u : 0u);
                 }
-                if (valid.x && u0.x < 0.0f) acc.clip -= u0.x;
-                if (valid.y && u0.y < 0.0f) acc.clip -= u0.y;
+                if (valid.x && u0.x < 0.0f) acc.clip -= (double)u0.x;
+                if (valid.y && u0.y < 0.0f) acc.clip -= (double)u0.y;
                 if (MASKED) {
-                    if (valid.x && !act.x) acc.mask += h.x;
-                    if (valid.y && !act.y) acc.mask += h.y;
+                    if (valid.x && !act.x) acc.mask += (double)h.x;
+                    if (valid.y && !act.y) acc.mask += (double)h.y;
                 }
             }
-            const int64_t so = (int64_t)r * p.out.pitch;
+            const int64_t so = (int64_t)r * out.pitch;
             if (c0 + 2 <= d.cols) {
-                *reinterpret_cast<float2*>(p.out.h + so + c0) = ho;
-                *reinterpret_cast<float2*>(p.out.hu + so + c0) = huo;
-                *reinterpret_cast<float2*>(p.out.hv + so + c0) = hvo;
+                *reinterpret_cast<float2*>(out.h + so + c0) = ho;
+                *reinterpret_cast<float2*>(out.hu + so + c0) = huo;
+                *reinterpret_cast<float2*>(out.hv + so + c0) = hvo;
             } else if (valid.x) {
-                p.out.h[so + c0] = ho.x;
-                p.out.hu[so + c0] = huo.x;
-                p.out.hv[so + c0] = hvo.x;
+                out.h[so + c0] = ho.x;
+                out.hu[so + c0] = huo.x;
+                out.hv[so + c0] = hvo.x;
             }
             if (RUN && snap >= 0) {
-                const Control* c = p.ctl;
+                const Control* c = ctl;
                 const int64_t base = (int64_t)snap * c->out_plane + (int64_t)r * d.cols + c0;
                 if (valid.x) {
                     c->out_h[base] = ho.x;
@@ -371,15 +358,106 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
         }
         cp_async_wait<0>();  // nothing may land after the warp is done
     }
+}
+
+template <class M, int THREADS, bool RUN, bool MASKED>
+__global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(const StepLaunch p) {
+    constexpr int NW = THREADS / kWarp;
+    __shared__ WarpSmem s_warp[NW];
+    const DomainDev& d = p.d;
+    StepScalars s = p.s;
+    int snap = -1;
+    double dtd = 0.0;
+    if constexpr (RUN) {
+        const Control* c = p.ctl;
+        if (*((volatile const int*)&c->done)) return;  // uniform early exit of the whole grid
+        s = c->s;
+        snap = c->snap;
+        dtd = c->dt;
+    }
+    const int wib = threadIdx.x >> 5;
+    const int gw = blockIdx.x * NW + wib;
+    const int strip = gw % p.nstrips;
+    const int chunk = gw / p.nstrips;
+    const int r0 = chunk * p.rows_per_warp;
+    const int r1 = min(r0 + p.rows_per_warp, d.rows);
+    StepAccum acc;
+    acc.zero();
+    if (r0 < d.rows)
+        march_pair<M, RUN, MASKED>(d, p.in, p.out, s, snap, dtd, p.ctl, r0, r1, strip * kWarp * 2,
+                                   s_warp[wib], acc);
     if constexpr (RUN) {
         Accum a;
         a.maxinv = acc.maxinv;
         a.vol = acc.vol;
-        a.rain = (double)acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
-        a.outflow = (double)acc.outflow;
-        a.clip = (double)acc.clip;
-        a.mask = (double)acc.mask;
+        a.rain = acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
+        a.outflow = acc.outflow;
+        a.clip = acc.clip;
+        a.mask = acc.mask;
         finish_run_step<THREADS>(d, p.ctl, p.parts, a, false);
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched ensemble: many domains of uneven size, one launch per step
+// ---------------------------------------------------------------------------
+// Each member is a complete domain (its own static planes, ping-pong state,
+// run control with float64 clock, CFL dt and mass ledger).  The launch's CTAs
+// are persistent: CTA b takes work items b, b + gridDim.x, ...; an item is one
+// CTA's worth of warps of one member (item.y = its slot among the member's
+// `ncta` slots).  After its march the CTA folds into that member's partials and
+// the member's last slot advances the member's clock and plans its next dt, so
+// members step with their own CFL dt and finish independently (a finished
+// member's items return at once).
+struct MemberDev {
+    DomainDev d;
+    float* buf[2][3];  // ping-pong h, hu, hv planes
+    int64_t pitch;
+    Control* ctl;
+    Partial* parts;
+    int nstrips, rows_per_warp, ncta;
+};
+
+template <class M, int THREADS, bool MASKED>
+__global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS)
+ensemble_step_kernel(const MemberDev* __restrict__ members, const int2* __restrict__ items,
+                     int n_items, int parity) {
+    constexpr int NW = THREADS / kWarp;
+    __shared__ WarpSmem s_warp[NW];
+    __shared__ MemberDev s_md;
+    const int wib = threadIdx.x >> 5;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const int2 item = items[it];
+        const Control* c = members[item.x].ctl;
+        if (*((volatile const int*)&c->done)) continue;  // uniform for the CTA
+        __syncthreads();  // the previous item is done with s_md
+        if (threadIdx.x == 0) s_md = members[item.x];
+        __syncthreads();
+        const MemberDev& md = s_md;
+        const StepScalars s = c->s;
+        const int snap = c->snap;
+        const double dtd = c->dt;
+        const int gw = item.y * NW + wib;
+        const int strip = gw % md.nstrips;
+        const int chunk = gw / md.nstrips;
+        const int r0 = chunk * md.rows_per_warp;
+        const int r1 = min(r0 + md.rows_per_warp, md.d.rows);
+        const StateView in{md.buf[parity][0], md.buf[parity][1], md.buf[parity][2], md.pitch};
+        const StateOut out{md.buf[parity ^ 1][0], md.buf[parity ^ 1][1], md.buf[parity ^ 1][2], md.pitch};
+        StepAccum acc;
+        acc.zero();
+        if (r0 < md.d.rows)
+            march_pair<M, true, MASKED>(md.d, in, out, s, snap, dtd, md.ctl, r0, r1, strip * kWarp * 2,
+                                        s_warp[wib], acc);
+        Accum a;
+        a.maxinv = acc.maxinv;
+        a.vol = acc.vol;
+        a.rain = acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
+        a.outflow = acc.outflow;
+        a.clip = acc.clip;
+        a.mask = acc.mask;
+        finish_run_step<THREADS>(md.d, md.ctl, md.parts, a, false, false, item.y, md.ncta);
     }
 }
 

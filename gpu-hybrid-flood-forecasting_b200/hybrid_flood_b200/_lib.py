@@ -37,6 +37,14 @@ EXPORTS = (
     "swe_set_timing",
     "swe_last_step_time",
     "swe_max_inverse_dt_noalloc",
+    "swe_ensemble_create",
+    "swe_ensemble_destroy",
+    "swe_ensemble_size",
+    "swe_ensemble_set_rows_per_warp",
+    "swe_ensemble_advance",
+    "swe_ensemble_set_timing",
+    "swe_ensemble_last_step_time",
+    "swe_ensemble_last_launch_count",
     "swe_last_error",
     "swe_version",
 )
@@ -112,6 +120,15 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_last_step_time": (ctypes.c_int, [_vp, ctypes.POINTER(_f64), ctypes.POINTER(_i64)]),
         "swe_max_inverse_dt_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _i32, _i32, _f64,
                                                       _f64, _f64, _f64, _vp, _vp]),
+        "swe_ensemble_create": (ctypes.c_int, [ctypes.POINTER(DomainDesc), _i32, ctypes.POINTER(_vp)]),
+        "swe_ensemble_destroy": (ctypes.c_int, [_vp]),
+        "swe_ensemble_size": (ctypes.c_int, [_vp]),
+        "swe_ensemble_set_rows_per_warp": (ctypes.c_int, [_vp, _i32]),
+        "swe_ensemble_advance": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp,
+                                                ctypes.POINTER(RunResult), _vp]),
+        "swe_ensemble_set_timing": (ctypes.c_int, [_vp, _i32]),
+        "swe_ensemble_last_step_time": (ctypes.c_int, [_vp, ctypes.POINTER(_f64), ctypes.POINTER(_i64)]),
+        "swe_ensemble_last_launch_count": (ctypes.c_int64, [_vp]),
         "swe_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
         "swe_version": (ctypes.c_char_p, []),
     }

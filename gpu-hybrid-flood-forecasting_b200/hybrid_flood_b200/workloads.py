@@ -170,9 +170,40 @@ def urban(rows: int = 2048, cols: int = 2048, *, dx: float = 1.0, seed: int = 1,
     )
 
 
-def ponded_initial_depth(workload: Workload, depth_m: float = 0.05) -> np.ndarray:
-    """A wet start: water at ``depth_m`` above the bed in every cell below the
-    90th-percentile bed elevation (the block tops stay dry)."""
-    bed = workload.bed
-    threshold = np.percentile(bed, 90.0)
-    return np.where(bed < threshold, depth_m, 0.0).astype(np.float32)
+ENSEMBLE_SHAPES = ((256, 256), (512, 512), (1024, 1024), (768, 1536))
+
+
+def ensemble_members(n: int = 64, *, seed: int = 2024, shapes=ENSEMBLE_SHAPES,
+                     rain_sigma_log: float = 0.4, n_range=(0.8, 1.2)) -> list[Workload]:
+    """The batched-ensemble case: ``n`` urban members of uneven size.
+
+    Member m uses DEM seed 1000 + m; its size is drawn uniformly from ``shapes``;
+    its rain is scaled by a LogNormal(0, sigma_log) factor and its Manning n by
+    U(n_range).  Expected total for 64 members: 64 x 638,976 = 40.9 M cells.
+    """
+    rng = np.random.default_rng(seed)
+    picks = rng.integers(0, len(shapes), n)
+    rain_f = rng.lognormal(0.0, rain_sigma_log, n)
+    n_f = rng.uniform(n_range[0], n_range[1], n)
+    out = []
+    for m in range(n):
+        rows, cols = shapes[int(picks[m])]
+        w = urban(rows, cols, seed=1000 + m, rain_scale=float(rain_f[m]), n_scale=float(n_f[m]))
+        w.name = f"member{m:02d}_{rows}x{cols}"
+        out.append(w)
+    return out
+
+
+def as_member(w: Workload) -> dict:
+    """Keyword arguments of one ensemble member (the B200ShallowWaterSolver constructor's)."""
+    return dict(bed=w.bed, manning_n=w.manning_n, domain_mask=w.domain_mask, **w.solver_kwargs())
+
+
+def street_depth(w: Workload, depth_m: float = 0.05) -> np.ndarray:
+    """Initial ponding of ``depth_m`` on the street cells of an urban workload
+    (cells within 1 m of the sloping plane; block tops stay dry)."""
+    rows, cols = w.shape
+    slope = float(w.meta.get("slope", 0.003))
+    x = (np.arange(cols, dtype=np.float64) + 0.5) * w.resolution_m
+    plane = slope * (cols * w.resolution_m - x)[None, :]
+    return np.where((w.bed - plane) < 1.0, depth_m, 0.0).astype(np.float32)

@@ -140,6 +140,32 @@ int swe_set_timing(swe_domain_t d, int32_t enable);
  * kernel of the last timed swe_run/swe_advance, and the step launches between. */
 int swe_last_step_time(swe_domain_t d, double *ms, int64_t *step_launches);
 
+/* ---- Batched ensemble (no single counterpart in the reference: it batches many
+ * reference runs -- NumpyShallowWaterSolver.run per member, numpy_solver/
+ * shallow_water_2d.py:382-424 -- into one launch per step). ---- */
+typedef struct swe_ensemble *swe_ensemble_t;
+
+/* Create an ensemble of n_members domains of any sizes (one swe_domain_desc
+ * each, all with the same arithmetic).  Every member keeps its own float64
+ * clock, CFL dt and mass ledger; one kernel launch advances all of them. */
+int swe_ensemble_create(const swe_domain_desc *descs, int32_t n_members, swe_ensemble_t *out);
+int swe_ensemble_destroy(swe_ensemble_t e);
+int swe_ensemble_size(swe_ensemble_t e);
+
+/* Rows each warp marches per work item (the tuning knob of the work list). */
+int swe_ensemble_set_rows_per_warp(swe_ensemble_t e, int32_t rows_per_warp);
+
+/* Advance every member IN PLACE by n_steps of its own CFL dt, starting at
+ * start_s[m] (NULL = 0).  h/hu/hv/pitch are arrays of n_members device
+ * pointers / pitches; results receives n_members entries. */
+int swe_ensemble_advance(swe_ensemble_t e, float *const *h, float *const *hu, float *const *hv,
+                         const int64_t *pitch, int32_t n_steps, const double *start_s,
+                         swe_run_result *results, void *stream);
+
+int swe_ensemble_set_timing(swe_ensemble_t e, int32_t enable);
+int swe_ensemble_last_step_time(swe_ensemble_t e, double *ms, int64_t *steps);
+int64_t swe_ensemble_last_launch_count(swe_ensemble_t e);
+
 /* Largest cell count swe_max_inverse_dt_noalloc accepts (a 4096 x 4096 grid). */
 #define SWE_NOALLOC_MAX_CELLS 16777216
 
