@@ -67,6 +67,8 @@ def _args():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-members", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=200)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -225,6 +227,50 @@ def _ensemble(args, dev, world: int):
     }
 
 
+def _adjoint(args, dev):
+    """Forward vs forward+adjoint time of the differentiable gauge rollout
+    (512x512, dx = 2 m, 2000 fixed-dt steps, gauges every 10 steps, checkpoint every 50)."""
+    import torch
+
+    from hybrid_flood_b200.adjoint import gauge_rollout
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver
+    from hybrid_flood_b200.workloads import adjoint_case
+
+    w, n_truth, n_est, gauges = adjoint_case(512, 512)
+    solver = B200ShallowWaterSolver(w.bed, n_est, w.domain_mask, **w.solver_kwargs(), arithmetic="exact",
+                                    device=dev)
+    depth = np.maximum(1.0 - w.bed, 0.2).astype(np.float32)
+    h0 = torch.tensor(depth, device=dev)
+    steps, dt = args.adjoint_steps, 0.2
+    kw = dict(n_steps=steps, dt=dt, gauge_index=gauges, obs_every=10, checkpoint_every=50)
+    with torch.no_grad():
+        obs = gauge_rollout(solver, torch.tensor(n_truth, device=dev), h0, 1.0, **kw)
+    n_t = torch.tensor(n_est, device=dev, requires_grad=True)
+    h_t = h0.clone().requires_grad_(True)
+    s_t = torch.tensor(1.0, device=dev, requires_grad=True)
+    stream = torch.cuda.current_stream(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    with torch.no_grad():
+        gauge_rollout(solver, n_t, h_t, s_t, **kw)  # warm-up
+    torch.cuda.synchronize(dev)
+    ev[0].record(stream)
+    with torch.no_grad():
+        gauge_rollout(solver, n_t, h_t, s_t, **kw)
+    ev[1].record(stream)
+    ev[2].record(stream)
+    pred = gauge_rollout(solver, n_t, h_t, s_t, **kw)
+    loss = torch.mean((pred - obs) ** 2)
+    loss.backward()
+    ev[3].record(stream)
+    torch.cuda.synchronize(dev)
+    f_ms = ev[0].elapsed_time(ev[1])
+    fb_ms = ev[2].elapsed_time(ev[3])
+    return {"workload": "512x512 dx=2m tilted plane + bumps, log-normal n (median 0.03, sigma_log 0.3, "
+                        "9-cell smoothing), 16 gauges every 10 steps, 2000 fixed-dt steps, checkpoint/50",
+            "steps": steps, "forward_ms": f_ms, "forward_adjoint_ms": fb_ms, "ratio": fb_ms / f_ms,
+            "loss": float(loss), "grad_n_norm": float(n_t.grad.norm()), "grad_rain_scale": float(s_t.grad)}
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
@@ -329,6 +375,9 @@ def run_b200(args, rank: int, world: int):
     ens = None
     if not args.no_ensemble:
         ens = _ensemble(args, dev, world)
+    adj = None
+    if not args.no_adjoint and rank == 0:
+        adj = _adjoint(args, dev)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -358,6 +407,8 @@ def run_b200(args, rank: int, world: int):
         line["e2e"] = e2e
     if ens:
         line["ensemble"] = ens
+    if adj:
+        line["adjoint"] = adj
     if not args.no_cpu_baseline:
         from oracle import cport
 

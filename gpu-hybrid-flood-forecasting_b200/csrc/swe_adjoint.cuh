@@ -1,0 +1,426 @@
+// Hand-written reverse mode (adjoint) of the shallow-water step (sm_100a).
+//
+// The reference has no adjoint: it never differentiates its solver (the only
+// gradients in it are of the U-Net, src/hybrid_flood/ml/train.py:181).  This is
+// the vector-Jacobian product of one step of
+// src/hybrid_flood/numpy_solver/shallow_water_2d.py:277-327 with dt held fixed
+// (a stop-gradient, as jax.grad of a fixed-dt scan would treat it):
+//
+//   given lambda' = dL/dU_{k+1}, returns lambda = dL/dU_k and accumulates
+//   dL/d(n^2) per cell and dL/d(rain scale).
+//
+// Non-smooth points use these conventions (zero where the forward is flat or
+// undefined): max(x, 0) passes the gradient only for x > 0; velocities m/h
+// only for h > dry; sqrt(g H) only for H > 0; the friction term's max(h, dry)
+// only for h > dry; hypot only for a non-zero norm; HLL speed min/max route to
+// the selected argument; the flux select follows the taken branch.
+//
+// Two kernels per reverse step:
+//   adj_cell_kernel  recomputes the cell's forward update (its four faces) and
+//                    reverses the pointwise part (rain, clip, friction, masks):
+//                    lambda_upd = dL/d(upd) per cell, plus the n^2 and rain
+//                    scale gradients;
+//   adj_face_kernel  gathers, for each cell, the flux VJPs of its four faces
+//                    (each face's flux depends on the states of its two cells
+//                    through reconstruction and HLL) into lambda = lambda_upd
+//                    + sum of face contributions.
+#pragma once
+
+#include "swe_step.cuh"
+
+namespace swe {
+
+struct AdjConsts {
+    float g, half_g, dry, eps, dx, dy;
+};
+
+struct FaceIn {
+    float h, hu, hv, z;
+    bool act;
+};
+
+__device__ __forceinline__ FaceIn face_in(const Cell& c) { return {c.h, c.hu, c.hv, c.z, active(c.nm)}; }
+
+// Forward flux of one face (plain float32 arithmetic; the adjoint needs the
+// values, not the reference's bit pattern).
+template <int AXIS>
+__device__ void adj_face_fwd(FaceIn lo, FaceIn hi, const AdjConsts& k, float F[3], float& clo, float& chi) {
+    F[0] = F[1] = F[2] = 0.f;
+    clo = chi = 0.f;
+    if (!(lo.act || hi.act)) return;
+    FaceIn L = lo, R = hi;
+    if (lo.act && !hi.act) {
+        R = lo;
+        if (AXIS == 1) R.hu = -lo.hu; else R.hv = -lo.hv;
+    } else if (!lo.act && hi.act) {
+        L = hi;
+        if (AXIS == 1) L.hu = -hi.hu; else L.hv = -hi.hv;
+    }
+    const float zf = fmaxf(L.z, R.z);
+    const float HL = fmaxf(L.h + L.z - zf, 0.f), HR = fmaxf(R.h + R.z - zf, 0.f);
+    const float uL = L.h > k.dry ? L.hu / L.h : 0.f, vL = L.h > k.dry ? L.hv / L.h : 0.f;
+    const float uR = R.h > k.dry ? R.hu / R.h : 0.f, vR = R.h > k.dry ? R.hv / R.h : 0.f;
+    const float XL = HL * uL, YL = HL * vL, XR = HR * uR, YR = HR * vR;
+    const float nL = AXIS == 1 ? XL : YL, nR = AXIS == 1 ? XR : YR;
+    const float unL = HL > k.dry ? nL / HL : 0.f, unR = HR > k.dry ? nR / HR : 0.f;
+    const float tL = HL > k.dry ? YL / HL : 0.f, tR = HR > k.dry ? YR / HR : 0.f;
+    const float cL = sqrtf(k.g * HL), cR = sqrtf(k.g * HR);
+    const float sL = fminf(unL - cL, unR - cR), sR = fmaxf(unL + cL, unR + cR);
+    const float pL = k.half_g * HL * HL, pR = k.half_g * HR * HR;
+    float fL[3], fR[3];
+    if (AXIS == 1) {
+        fL[0] = XL; fL[1] = XL * unL + pL; fL[2] = XL * tL;
+        fR[0] = XR; fR[1] = XR * unR + pR; fR[2] = XR * tR;
+    } else {
+        fL[0] = YL; fL[1] = XL * unL; fL[2] = YL * unL + pL;
+        fR[0] = YR; fR[1] = XR * unR; fR[2] = YR * unR + pR;
+    }
+    const float UL[3] = {HL, XL, YL}, UR[3] = {HR, XR, YR};
+    const float spread = sR - sL;
+    const float den = spread > k.eps ? spread : 1.f;
+    for (int q = 0; q < 3; ++q) {
+        const float m = (sR * fL[q] - sL * fR[q] + sL * sR * (UR[q] - UL[q])) / den;
+        F[q] = sL >= 0.f ? fL[q] : (sR <= 0.f ? fR[q] : m);
+    }
+    clo = k.half_g * (L.h * L.h - HL * HL);
+    chi = k.half_g * (R.h * R.h - HR * HR);
+}
+
+// VJP of one face: given dL/dF (3), dL/dcorr_lo, dL/dcorr_hi, return dL/d(h, hu, hv)
+// of the lo cell and of the hi cell (after undoing the wall mirroring).
+template <int AXIS>
+__device__ void adj_face_vjp(FaceIn lo, FaceIn hi, const AdjConsts& k, const float lF[3], float lclo,
+                             float lchi, float dlo[3], float dhi[3]) {
+    dlo[0] = dlo[1] = dlo[2] = 0.f;
+    dhi[0] = dhi[1] = dhi[2] = 0.f;
+    if (!(lo.act || hi.act)) return;
+    const bool hi_wall = lo.act && !hi.act, lo_wall = !lo.act && hi.act;
+    FaceIn L = lo, R = hi;
+    if (hi_wall) {
+        R = lo;
+        if (AXIS == 1) R.hu = -lo.hu; else R.hv = -lo.hv;
+    } else if (lo_wall) {
+        L = hi;
+        if (AXIS == 1) L.hu = -hi.hu; else L.hv = -hi.hv;
+    }
+    // ---- forward, keeping what the reverse needs ----
+    const float zf = fmaxf(L.z, R.z);
+    const float aL = L.h + L.z - zf, aR = R.h + R.z - zf;
+    const float HL = fmaxf(aL, 0.f), HR = fmaxf(aR, 0.f);
+    const bool dL = L.h > k.dry, dR = R.h > k.dry;
+    const float uL = dL ? L.hu / L.h : 0.f, vL = dL ? L.hv / L.h : 0.f;
+    const float uR = dR ? R.hu / R.h : 0.f, vR = dR ? R.hv / R.h : 0.f;
+    const float XL = HL * uL, YL = HL * vL, XR = HR * uR, YR = HR * vR;
+    const float nL = AXIS == 1 ? XL : YL, nR = AXIS == 1 ? XR : YR;
+    const bool wL = HL > k.dry, wR = HR > k.dry;
+    const float unL = wL ? nL / HL : 0.f, unR = wR ? nR / HR : 0.f;
+    const float tL = wL ? YL / HL : 0.f, tR = wR ? YR / HR : 0.f;
+    const float cL = sqrtf(k.g * HL), cR = sqrtf(k.g * HR);
+    const float aminL = unL - cL, aminR = unR - cR, amaxL = unL + cL, amaxR = unR + cR;
+    const float sL = fminf(aminL, aminR), sR = fmaxf(amaxL, amaxR);
+    const float pL = k.half_g * HL * HL, pR = k.half_g * HR * HR;
+    float fL[3], fR[3];
+    if (AXIS == 1) {
+        fL[0] = XL; fL[1] = XL * unL + pL; fL[2] = XL * tL;
+        fR[0] = XR; fR[1] = XR * unR + pR; fR[2] = XR * tR;
+    } else {
+        fL[0] = YL; fL[1] = XL * unL; fL[2] = YL * unL + pL;
+        fR[0] = YR; fR[1] = XR * unR; fR[2] = YR * unR + pR;
+    }
+    const float UL[3] = {HL, XL, YL}, UR[3] = {HR, XR, YR};
+    const float spread = sR - sL;
+    const bool use_spread = spread > k.eps;
+    const float den = use_spread ? spread : 1.f;
+    const bool take_l = sL >= 0.f, take_r = !take_l && sR <= 0.f;
+    // ---- reverse ----
+    float lfL[3] = {0.f, 0.f, 0.f}, lfR[3] = {0.f, 0.f, 0.f};
+    float lUL[3] = {0.f, 0.f, 0.f}, lUR[3] = {0.f, 0.f, 0.f};
+    float lsL = 0.f, lsR = 0.f;
+    if (take_l) {
+        for (int q = 0; q < 3; ++q) lfL[q] = lF[q];
+    } else if (take_r) {
+        for (int q = 0; q < 3; ++q) lfR[q] = lF[q];
+    } else {
+        float lden = 0.f;
+        for (int q = 0; q < 3; ++q) {
+            const float dU = UR[q] - UL[q];
+            const float m = (sR * fL[q] - sL * fR[q] + sL * sR * dU) / den;
+            const float lN = lF[q] / den;
+            lden -= m * lN;
+            lsR += (fL[q] + sL * dU) * lN;
+            lsL += (-fR[q] + sR * dU) * lN;
+            lfL[q] += sR * lN;
+            lfR[q] -= sL * lN;
+            lUR[q] += sL * sR * lN;
+            lUL[q] -= sL * sR * lN;
+        }
+        if (use_spread) {
+            lsR += lden;
+            lsL -= lden;
+        }
+    }
+    // corrections: half_g (h^2 - H^2) on each side
+    float lLh = k.g * L.h * lclo, lRh = k.g * R.h * lchi;
+    float lHL = lUL[0] - k.g * HL * lclo, lHR = lUR[0] - k.g * HR * lchi;
+    float lXL = lUL[1], lYL = lUL[2], lXR = lUR[1], lYR = lUR[2];
+    float lunL = 0.f, lunR = 0.f, ltL = 0.f, ltR = 0.f, lpL = 0.f, lpR = 0.f;
+    if (AXIS == 1) {
+        lXL += lfL[0] + unL * lfL[1] + tL * lfL[2];
+        lunL += XL * lfL[1];
+        lpL += lfL[1];
+        ltL += XL * lfL[2];
+        lXR += lfR[0] + unR * lfR[1] + tR * lfR[2];
+        lunR += XR * lfR[1];
+        lpR += lfR[1];
+        ltR += XR * lfR[2];
+    } else {
+        lYL += lfL[0] + unL * lfL[2];
+        lXL += unL * lfL[1];
+        lunL += XL * lfL[1] + YL * lfL[2];
+        lpL += lfL[2];
+        lYR += lfR[0] + unR * lfR[2];
+        lXR += unR * lfR[1];
+        lunR += XR * lfR[1] + YR * lfR[2];
+        lpR += lfR[2];
+    }
+    lHL += k.g * HL * lpL;
+    lHR += k.g * HR * lpR;
+    // wave speeds: min/max route to the selected argument
+    float lcL = 0.f, lcR = 0.f;
+    if (aminL <= aminR) { lunL += lsL; lcL -= lsL; } else { lunR += lsL; lcR -= lsL; }
+    if (amaxL >= amaxR) { lunL += lsR; lcL += lsR; } else { lunR += lsR; lcR += lsR; }
+    if (cL > 0.f) lHL += 0.5f * k.g / cL * lcL;
+    if (cR > 0.f) lHR += 0.5f * k.g / cR * lcR;
+    // un = n / H, t = Y / H (for H > dry)
+    float lnL = 0.f, lnR = 0.f;
+    if (wL) {
+        lnL += lunL / HL;
+        lHL -= unL / HL * lunL;
+        if (AXIS == 1) {
+            lYL += ltL / HL;
+            lHL -= tL / HL * ltL;
+        }
+    }
+    if (wR) {
+        lnR += lunR / HR;
+        lHR -= unR / HR * lunR;
+        if (AXIS == 1) {
+            lYR += ltR / HR;
+            lHR -= tR / HR * ltR;
+        }
+    }
+    if (AXIS == 1) { lXL += lnL; lXR += lnR; } else { lYL += lnL; lYR += lnR; }
+    // X = H u, Y = H v
+    lHL += uL * lXL + vL * lYL;
+    lHR += uR * lXR + vR * lYR;
+    const float luL = HL * lXL, lvL = HL * lYL, luR = HR * lXR, lvR = HR * lYR;
+    // H = max(h + z - zf, 0) with the bed held fixed
+    if (aL > 0.f) lLh += lHL;
+    if (aR > 0.f) lRh += lHR;
+    // u = hu / h, v = hv / h (for h > dry)
+    float gL[3] = {lLh, 0.f, 0.f}, gR[3] = {lRh, 0.f, 0.f};
+    if (dL) {
+        gL[1] = luL / L.h;
+        gL[2] = lvL / L.h;
+        gL[0] -= (uL * luL + vL * lvL) / L.h;
+    }
+    if (dR) {
+        gR[1] = luR / R.h;
+        gR[2] = lvR / R.h;
+        gR[0] -= (uR * luR + vR * lvR) / R.h;
+    }
+    // undo the wall mirroring: the mirrored side's gradient belongs to the active cell
+    const int nq = AXIS == 1 ? 1 : 2;
+    if (hi_wall) {
+        for (int q = 0; q < 3; ++q) dlo[q] = gL[q] + (q == nq ? -gR[q] : gR[q]);
+    } else if (lo_wall) {
+        for (int q = 0; q < 3; ++q) dhi[q] = gR[q] + (q == nq ? -gL[q] : gL[q]);
+    } else {
+        for (int q = 0; q < 3; ++q) {
+            dlo[q] = gL[q];
+            dhi[q] = gR[q];
+        }
+    }
+}
+
+struct AdjLaunch {
+    DomainDev d;
+    StateView in;        // U_k
+    StateView lam;       // dL/dU_{k+1}
+    StateOut lam_out;    // dL/dU_k
+    float* lupd[3];      // scratch: dL/d(upd) planes, pitch lpitch
+    int64_t lpitch;
+    float* grad_n2;      // rows x cols, accumulated
+    double* grad_rain;   // device scalar, accumulated
+    StepScalars s;       // float32 dt, dt*rate (scaled), dt*g
+    float dt_rate;       // float32 dt * rate(t) before the rain scale
+    AdjConsts k;
+};
+
+__device__ __forceinline__ Cell adj_load(const DomainDev& d, const StateView& s, int r, int c) {
+    Cell t[1];
+    load_cells<1>(d, s, r, c, t);
+    return t[0];
+}
+
+// The forward update of cell (r, c) from its four faces: upd (3) before the
+// pointwise part.
+__device__ void adj_cell_update(const AdjLaunch& p, int r, int c, float upd[3]) {
+    const DomainDev& d = p.d;
+    const FaceIn C = face_in(adj_load(d, p.in, r, c));
+    const FaceIn W = face_in(adj_load(d, p.in, r, c - 1)), E = face_in(adj_load(d, p.in, r, c + 1));
+    const FaceIn S = face_in(adj_load(d, p.in, r - 1, c)), N = face_in(adj_load(d, p.in, r + 1, c));
+    float Fl[3], Fr[3], Fb[3], Ft[3], cl_lo, cl_hi, cr_lo, cr_hi, cb_lo, cb_hi, ct_lo, ct_hi;
+    adj_face_fwd<1>(W, C, p.k, Fl, cl_lo, cl_hi);
+    adj_face_fwd<1>(C, E, p.k, Fr, cr_lo, cr_hi);
+    adj_face_fwd<0>(S, C, p.k, Fb, cb_lo, cb_hi);
+    adj_face_fwd<0>(C, N, p.k, Ft, ct_lo, ct_hi);
+    const float U[3] = {C.h, C.hu, C.hv};
+    for (int q = 0; q < 3; ++q) {
+        const float xl = Fr[q] + (q == 1 ? cr_lo : 0.f);
+        const float xr = Fl[q] + (q == 1 ? cl_hi : 0.f);
+        const float yb = Ft[q] + (q == 2 ? ct_lo : 0.f);
+        const float yt = Fb[q] + (q == 2 ? cb_hi : 0.f);
+        upd[q] = U[q] - p.s.dt * ((xl - xr) / p.k.dx + (yb - yt) / p.k.dy);
+    }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) adj_cell_kernel(const AdjLaunch p) {
+    const DomainDev& d = p.d;
+    const int64_t n = (int64_t)d.rows * d.cols;
+    double rain_acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * THREADS) {
+        const int r = (int)(i / d.cols), c = (int)(i - (int64_t)r * d.cols);
+        const float nm = d.nm[(int64_t)r * d.spitch + c];
+        const bool act = active(nm);
+        const int64_t lo = (int64_t)r * p.lpitch + c;
+        if (!act) {
+            p.lupd[0][lo] = p.lupd[1][lo] = p.lupd[2][lo] = 0.f;
+            continue;
+        }
+        float upd[3];
+        adj_cell_update(p, r, c, upd);
+        const float mult = d.mult ? d.mult[(int64_t)r * d.spitch + c] : 1.f;
+        upd[0] += p.s.dt_rain * mult;
+        const float h = fmaxf(upd[0], 0.f);
+        const float norm = sqrtf(upd[1] * upd[1] + upd[2] * upd[2]);
+        const float m = fmaxf(h, p.k.dry);
+        const float pw = powf(m, -7.0f / 3.0f);
+        const float n2 = fabsf(nm);
+        const float fr = p.s.dt_g * n2 * norm * pw;
+        const float den = 1.f + fr;
+        const float qx = upd[1] / den, qy = upd[2] / den;
+        const bool wet = h > p.k.dry;
+        const int64_t li = (int64_t)r * p.lam.pitch + c;
+        const float lqx = wet ? p.lam.hu[li] : 0.f, lqy = wet ? p.lam.hv[li] : 0.f;
+        float lh = p.lam.h[li];
+        const float lden = -(lqx * qx + lqy * qy) / den;
+        float lu1 = lqx / den, lu2 = lqy / den;
+        if (norm > 0.f) {
+            const float lnorm = lden * p.s.dt_g * n2 * pw;
+            lu1 += lnorm * upd[1] / norm;
+            lu2 += lnorm * upd[2] / norm;
+        }
+        p.grad_n2[(int64_t)r * d.cols + c] += lden * p.s.dt_g * norm * pw;
+        if (h > p.k.dry) lh += lden * fr * (-7.0f / 3.0f) / h;
+        const float lu0 = upd[0] > 0.f ? lh : 0.f;
+        rain_acc += (double)lu0 * (double)p.dt_rate * (double)mult;
+        p.lupd[0][lo] = lu0;
+        p.lupd[1][lo] = lu1;
+        p.lupd[2][lo] = lu2;
+    }
+    rain_acc = warp_sum(rain_acc);
+    __shared__ double s_r[THREADS / kWarp];
+    if ((threadIdx.x & 31) == 0) s_r[threadIdx.x >> 5] = rain_acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < THREADS / kWarp; ++w) t += s_r[w];
+        if (t != 0.0) atomicAdd(p.grad_rain, t);
+    }
+}
+
+// dL/d(upd) of cell (r, c); zero outside the grid (ghost cells are not updated).
+__device__ __forceinline__ void lupd_at(const AdjLaunch& p, int r, int c, float l[3]) {
+    if (r < 0 || r >= p.d.rows || c < 0 || c >= p.d.cols) {
+        l[0] = l[1] = l[2] = 0.f;
+        return;
+    }
+    const int64_t o = (int64_t)r * p.lpitch + c;
+    l[0] = p.lupd[0][o];
+    l[1] = p.lupd[1][o];
+    l[2] = p.lupd[2][o];
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) adj_face_kernel(const AdjLaunch p) {
+    const DomainDev& d = p.d;
+    const int64_t n = (int64_t)d.rows * d.cols;
+    const float ax = p.s.dt / p.k.dx, ay = p.s.dt / p.k.dy;
+    for (int64_t i = (int64_t)blockIdx.x * THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * THREADS) {
+        const int r = (int)(i / d.cols), c = (int)(i - (int64_t)r * d.cols);
+        float g[3];
+        lupd_at(p, r, c, g);  // upd_q = U_q - ... : direct term
+        const FaceIn C = face_in(adj_load(d, p.in, r, c));
+        float lc[3], lo_[3], dlo[3], dhi[3], lF[3];
+        // right x-face (C | E): C is the lo side
+        {
+            const FaceIn E = face_in(adj_load(d, p.in, r, c + 1));
+            lupd_at(p, r, c + 1, lo_);
+            lupd_at(p, r, c, lc);
+            for (int q = 0; q < 3; ++q) lF[q] = -ax * lc[q] + ax * lo_[q];
+            adj_face_vjp<1>(C, E, p.k, lF, -ax * lc[1], ax * lo_[1], dlo, dhi);
+            for (int q = 0; q < 3; ++q) g[q] += dlo[q];
+            if (c == d.cols - 1) {  // E is the ghost copy of C
+                const float s = d.bnd[1] == 0 ? -1.f : 1.f;
+                g[0] += dhi[0]; g[1] += s * dhi[1]; g[2] += dhi[2];
+            }
+        }
+        // left x-face (W | C): C is the hi side
+        {
+            const FaceIn W = face_in(adj_load(d, p.in, r, c - 1));
+            lupd_at(p, r, c - 1, lo_);
+            lupd_at(p, r, c, lc);
+            for (int q = 0; q < 3; ++q) lF[q] = -ax * lo_[q] + ax * lc[q];
+            adj_face_vjp<1>(W, C, p.k, lF, -ax * lo_[1], ax * lc[1], dlo, dhi);
+            for (int q = 0; q < 3; ++q) g[q] += dhi[q];
+            if (c == 0) {
+                const float s = d.bnd[0] == 0 ? -1.f : 1.f;
+                g[0] += dlo[0]; g[1] += s * dlo[1]; g[2] += dlo[2];
+            }
+        }
+        // top y-face (C | N): C is the lo side
+        {
+            const FaceIn N = face_in(adj_load(d, p.in, r + 1, c));
+            lupd_at(p, r + 1, c, lo_);
+            lupd_at(p, r, c, lc);
+            for (int q = 0; q < 3; ++q) lF[q] = -ay * lc[q] + ay * lo_[q];
+            adj_face_vjp<0>(C, N, p.k, lF, -ay * lc[2], ay * lo_[2], dlo, dhi);
+            for (int q = 0; q < 3; ++q) g[q] += dlo[q];
+            if (r == d.rows - 1) {
+                const float s = d.bnd[3] == 0 ? -1.f : 1.f;
+                g[0] += dhi[0]; g[1] += dhi[1]; g[2] += s * dhi[2];
+            }
+        }
+        // bottom y-face (S | C): C is the hi side
+        {
+            const FaceIn S = face_in(adj_load(d, p.in, r - 1, c));
+            lupd_at(p, r - 1, c, lo_);
+            lupd_at(p, r, c, lc);
+            for (int q = 0; q < 3; ++q) lF[q] = -ay * lo_[q] + ay * lc[q];
+            adj_face_vjp<0>(S, C, p.k, lF, -ay * lo_[2], ay * lc[2], dlo, dhi);
+            for (int q = 0; q < 3; ++q) g[q] += dhi[q];
+            if (r == 0) {
+                const float s = d.bnd[2] == 0 ? -1.f : 1.f;
+                g[0] += dlo[0]; g[1] += dlo[1]; g[2] += s * dlo[2];
+            }
+        }
+        const int64_t o = (int64_t)r * p.lam_out.pitch + c;
+        p.lam_out.h[o] = g[0];
+        p.lam_out.hu[o] = g[1];
+        p.lam_out.hv[o] = g[2];
+    }
+}
+
+}  // namespace swe

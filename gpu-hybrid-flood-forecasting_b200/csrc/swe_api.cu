@@ -19,6 +19,7 @@
 #include "swe_b200.h"
 #include "swe_step.cuh"
 #include "swe_step_pair.cuh"
+#include "swe_adjoint.cuh"
 
 using namespace swe;
 
@@ -105,6 +106,9 @@ struct swe_domain {
     int rows_per_warp_override = 0;
     int run_vec = 2;     // lane width of the run-mode kernel (SWE_RUN_VEC=1|2)
     bool masked = true;  // false when every cell is active (mask-free kernels)
+    int occ_cache[2][2] = {{0, 0}, {0, 0}};  // [V-1][run]: CTAs per SM of the step kernels
+    float* lupd[3] = {nullptr, nullptr, nullptr};  // adjoint scratch
+    int64_t lpitch = 0;
 };
 
 namespace {
@@ -158,13 +162,17 @@ Plan make_plan(const swe_domain* d, int V, bool run) {
     p.V = V;
     const int rows = d->dd.rows, cols = d->dd.cols;
     p.nstrips = (cols + kWarp * V - 1) / (kWarp * V);
-    int occ = 1;
-    auto occ_of = [&](auto k) {
-        int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, decltype(k)::fn(), kThreads, 0) == cudaSuccess && n > 0)
-            occ = n;
-    };
-    dispatch(V, d->arith, run, d->masked, occ_of);
+    // The occupancy query costs more than a small step: ask once per kernel instance.
+    int& occ = const_cast<swe_domain*>(d)->occ_cache[V - 1][run ? 1 : 0];
+    if (occ <= 0) {
+        occ = 1;
+        auto occ_of = [&](auto k) {
+            int n = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, decltype(k)::fn(), kThreads, 0) == cudaSuccess && n > 0)
+                occ = n;
+        };
+        dispatch(V, d->arith, run, d->masked, occ_of);
+    }
     const int wpb = kThreads / kWarp;
     const int64_t warps_avail = (int64_t)occ * d->sms * wpb;
     int R = d->rows_per_warp_override;
@@ -371,6 +379,7 @@ void free_domain(swe_domain* d) {
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 3; ++f) cudaFree(d->ping[b][f]);
     cudaFree(d->times_dev);
+    for (int q = 0; q < 3; ++q) cudaFree(d->lupd[q]);
     for (int i = 0; i < 2; ++i) {
         if (d->poll_ev[i]) cudaEventDestroy(d->poll_ev[i]);
         if (d->time_ev[i]) cudaEventDestroy(d->time_ev[i]);
@@ -636,6 +645,42 @@ int noalloc_scratch(NoAllocScratch** out) {
 
 }  // namespace
 
+namespace {
+// Depth at flat cell indices (rows*cols numbering) of a pitched plane.
+__global__ void gauge_gather_kernel(const float* h, int64_t pitch, int cols, const int64_t* idx, int n,
+                                    float* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int64_t k = idx[i];
+        out[i] = h[(k / cols) * pitch + (k % cols)];
+    }
+}
+
+// lam_h[idx[i]] += g[i] (atomic: gauges may repeat).
+__global__ void gauge_inject_kernel(float* lam_h, int64_t pitch, int cols, const int64_t* idx, int n,
+                                    const float* g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int64_t k = idx[i];
+        atomicAdd(&lam_h[(k / cols) * pitch + (k % cols)], g[i]);
+    }
+}
+
+// Replace n^2 in the packed plane, keeping the mask in the sign bit.
+__global__ void repack_manning_kernel(const float* n, int rows, int cols, int64_t pitch, float* nm) {
+    const int64_t total = (int64_t)rows * pitch;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / pitch), c = (int)(i - (int64_t)r * pitch);
+        const int cc = c < cols ? c : cols - 1;
+        const float v = n[(int64_t)r * cols + cc];
+        const float n2 = fabsf(__fmul_rn(v, v));
+        const bool inactive = signbit(nm[i]);
+        nm[i] = inactive ? __int_as_float(__float_as_int(n2) | (int)0x80000000) : n2;
+    }
+}
+}  // namespace
+
 extern "C" {
 
 const char* swe_version(void) { return "swe_b200 0.1.0 sm_100a"; }
@@ -776,6 +821,7 @@ int swe_domain_create(const swe_domain_desc* desc, swe_domain_t* out) {
     dd.rain_t = d->rain;
     dd.rain_r = d->rain + q.n_rain;
     dd.n_rain = q.n_rain;
+    dd.rain_scale = 1.0;
     *out = d;
     return SWE_OK;
 }
@@ -789,7 +835,78 @@ int swe_domain_destroy(swe_domain_t d) {
 
 int swe_rainfall_rate(swe_domain_t d, double time_s, double* rate_out) {
     if (!d || !rate_out) return fail(SWE_ERR_INVALID, "null argument");
-    *rate_out = host_rain_rate(d->rain_t, d->rain_r, d->dd.default_rain, time_s);
+    *rate_out = d->dd.rain_scale * host_rain_rate(d->rain_t, d->rain_r, d->dd.default_rain, time_s);
+    return SWE_OK;
+}
+
+int swe_domain_set_rain_scale(swe_domain_t d, double scale) {
+    if (!d) return fail(SWE_ERR_INVALID, "null domain");
+    if (!(scale >= 0.0) || !std::isfinite(scale)) return fail(SWE_ERR_INVALID, "rain scale must be finite and >= 0");
+    d->dd.rain_scale = scale;
+    return SWE_OK;
+}
+
+int swe_domain_set_manning(swe_domain_t d, const float* manning_n, int32_t on_host, void* stream) {
+    if (!d || !manning_n) return fail(SWE_ERR_INVALID, "null argument");
+    const int rows = d->dd.rows, cols = d->dd.cols;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float* src = manning_n;
+    float* staged = nullptr;
+    if (on_host) {
+        SWE_CK(cudaMalloc(&staged, sizeof(float) * (size_t)rows * cols));
+        SWE_CK(cudaMemcpyAsync(staged, manning_n, sizeof(float) * (size_t)rows * cols, cudaMemcpyHostToDevice, st));
+        src = staged;
+    }
+    const int64_t n = (int64_t)rows * d->dd.spitch;
+    repack_manning_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(src, rows, cols, d->dd.spitch, d->nm);
+    SWE_CK(cudaGetLastError());
+    if (staged) {
+        SWE_CK(cudaStreamSynchronize(st));
+        cudaFree(staged);
+    }
+    return SWE_OK;
+}
+
+int swe_adjoint_step(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch,
+                     const float* lam_h, const float* lam_hu, const float* lam_hv, int64_t lam_pitch,
+                     float* lam_h_out, float* lam_hu_out, float* lam_hv_out, int64_t out_pitch,
+                     float* grad_n2, double* grad_rain_scale, double dt, double time_s, void* stream) {
+    if (!d || !grad_n2 || !grad_rain_scale) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    rc = check_state_ptrs(lam_h, lam_hu, lam_hv, lam_pitch, d->dd.cols);
+    if (rc) return rc;
+    rc = check_state_ptrs(lam_h_out, lam_hu_out, lam_hv_out, out_pitch, d->dd.cols);
+    if (rc) return rc;
+    const int rows = d->dd.rows;
+    if (!d->lupd[0]) {
+        d->lpitch = round_up(d->dd.cols, 128);
+        for (int q = 0; q < 3; ++q) SWE_CK(cudaMalloc(&d->lupd[q], sizeof(float) * (size_t)d->lpitch * rows));
+    }
+    const double rate = host_rain_rate(d->rain_t, d->rain_r, d->dd.default_rain, time_s);
+    AdjLaunch al{};
+    al.d = d->dd;
+    al.in = StateView{h, hu, hv, pitch};
+    al.lam = StateView{lam_h, lam_hu, lam_hv, lam_pitch};
+    al.lam_out = StateOut{lam_h_out, lam_hu_out, lam_hv_out, out_pitch};
+    for (int q = 0; q < 3; ++q) al.lupd[q] = d->lupd[q];
+    al.lpitch = d->lpitch;
+    al.grad_n2 = grad_n2;
+    al.grad_rain = grad_rain_scale;
+    al.s.dt = (float)dt;
+    const volatile double dr = dt * (d->dd.rain_scale * rate);
+    const volatile double dg = dt * d->dd.g;
+    const volatile double dru = dt * rate;
+    al.s.dt_rain = (float)dr;
+    al.s.dt_g = (float)dg;
+    al.dt_rate = (float)dru;
+    al.k = AdjConsts{d->dd.k.g, d->dd.k.half_g, d->dd.k.dry, d->dd.k.eps, d->dd.k.dx, d->dd.k.dy};
+    const int64_t n = (int64_t)rows * d->dd.cols;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + kThreads - 1) / kThreads, (int64_t)d->sms * 16));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    adj_cell_kernel<kThreads><<<blocks, kThreads, 0, st>>>(al);
+    adj_face_kernel<kThreads><<<blocks, kThreads, 0, st>>>(al);
+    SWE_CK(cudaGetLastError());
     return SWE_OK;
 }
 
@@ -809,7 +926,7 @@ int swe_step(swe_domain_t d, const float* h, const float* hu, const float* hv, i
     const void* all[6] = {h, hu, hv, h_out, hu_out, hv_out};
     const int V = choose_vec(all, 6, pitch_in, pitch_out);
     const Plan pl = make_plan(d, V, false);
-    const double rate = host_rain_rate(d->rain_t, d->rain_r, d->dd.default_rain, time_s);
+    const volatile double rate = d->dd.rain_scale * host_rain_rate(d->rain_t, d->rain_r, d->dd.default_rain, time_s);
     StepLaunch sl{};
     sl.d = d->dd;
     sl.in = StateView{h, hu, hv, pitch_in};
@@ -919,6 +1036,99 @@ int swe_advance(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, i
 }
 
 int64_t swe_last_launch_count(swe_domain_t d) { return d ? d->launches : -1; }
+
+int swe_rollout_forward(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, int32_t n_steps,
+                        double dt, double t0, const int64_t* gauge_index, int32_t n_gauges,
+                        int32_t obs_every, float* obs, float* ckpt, int32_t ckpt_every, void* stream) {
+    if (!d) return fail(SWE_ERR_INVALID, "null domain");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    if (n_steps < 0 || (n_gauges > 0 && (!gauge_index || !obs || obs_every < 1)) || (ckpt && ckpt_every < 1))
+        return fail(SWE_ERR_INVALID, "bad rollout arguments");
+    rc = ensure_ping(d);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int rows = d->dd.rows, cols = d->dd.cols;
+    float* user[3] = {h, hu, hv};
+    for (int f = 0; f < 3; ++f) {
+        rc = copy_plane(d->ping[0][f], d->ppitch, user[f], pitch, rows, cols, st);
+        if (rc) return rc;
+    }
+    const int64_t plane = (int64_t)rows * cols;
+    double t = t0;
+    for (int k = 0; k < n_steps; ++k) {
+        const int src = k & 1;
+        if (ckpt && k % ckpt_every == 0) {
+            float* dst = ckpt + (int64_t)(k / ckpt_every) * 3 * plane;
+            for (int f = 0; f < 3; ++f) {
+                rc = copy_plane(dst + f * plane, cols, d->ping[src][f], d->ppitch, rows, cols, st);
+                if (rc) return rc;
+            }
+        }
+        rc = swe_step(d, d->ping[src][0], d->ping[src][1], d->ping[src][2], d->ppitch, d->ping[src ^ 1][0],
+                      d->ping[src ^ 1][1], d->ping[src ^ 1][2], d->ppitch, dt, t, stream);
+        if (rc) return rc;
+        t += dt;
+        if (n_gauges > 0 && (k + 1) % obs_every == 0) {
+            gauge_gather_kernel<<<(n_gauges + 127) / 128, 128, 0, st>>>(
+                d->ping[src ^ 1][0], d->ppitch, cols, gauge_index, n_gauges,
+                obs + (int64_t)((k + 1) / obs_every - 1) * n_gauges);
+        }
+    }
+    const int fb = n_steps & 1;
+    for (int f = 0; f < 3; ++f) {
+        rc = copy_plane(user[f], pitch, d->ping[fb][f], d->ppitch, rows, cols, st);
+        if (rc) return rc;
+    }
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
+int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, int32_t n_steps, double dt,
+                         double t0, const int64_t* gauge_index, int32_t n_gauges, int32_t obs_every,
+                         const float* grad_obs, float* lam_h, float* lam_hu, float* lam_hv, int64_t lam_pitch,
+                         float* grad_n2, double* grad_rain_scale, float* seg, void* stream) {
+    if (!d || !ckpt || !seg || ckpt_every < 1 || n_steps < 0) return fail(SWE_ERR_INVALID, "bad rollout arguments");
+    if (n_gauges > 0 && (!gauge_index || !grad_obs || obs_every < 1)) return fail(SWE_ERR_INVALID, "bad gauge arguments");
+    int rc = check_state_ptrs(lam_h, lam_hu, lam_hv, lam_pitch, d->dd.cols);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int rows = d->dd.rows, cols = d->dd.cols;
+    const int64_t plane = (int64_t)rows * cols;
+    float* lam[3] = {lam_h, lam_hu, lam_hv};
+    for (int f = 0; f < 3; ++f)
+        SWE_CK(cudaMemset2DAsync(lam[f], sizeof(float) * lam_pitch, 0, sizeof(float) * cols, rows, st));
+    const int nseg = n_steps > 0 ? (n_steps + ckpt_every - 1) / ckpt_every : 0;
+    for (int sgi = nseg - 1; sgi >= 0; --sgi) {
+        const int k0 = sgi * ckpt_every;
+        const int k1 = std::min(k0 + ckpt_every, n_steps);
+        // Recompute the segment's states U_k0 .. U_{k1-1} into seg[0 .. k1-k0-1].
+        SWE_CK(cudaMemcpyAsync(seg, ckpt + (int64_t)sgi * 3 * plane, sizeof(float) * 3 * plane,
+                               cudaMemcpyDeviceToDevice, st));
+        for (int k = k0; k < k1 - 1; ++k) {
+            const float* a = seg + (int64_t)(k - k0) * 3 * plane;
+            float* b = seg + (int64_t)(k + 1 - k0) * 3 * plane;
+            rc = swe_step(d, a, a + plane, a + 2 * plane, cols, b, b + plane, b + 2 * plane, cols, dt,
+                          t0 + k * dt, stream);
+            if (rc) return rc;
+        }
+        for (int k = k1 - 1; k >= k0; --k) {
+            if (n_gauges > 0 && (k + 1) % obs_every == 0) {
+                gauge_inject_kernel<<<(n_gauges + 127) / 128, 128, 0, st>>>(
+                    lam_h, lam_pitch, cols, gauge_index, n_gauges,
+                    grad_obs + (int64_t)((k + 1) / obs_every - 1) * n_gauges);
+            }
+            const float* a = seg + (int64_t)(k - k0) * 3 * plane;
+            rc = swe_adjoint_step(d, a, a + plane, a + 2 * plane, cols, lam_h, lam_hu, lam_hv, lam_pitch,
+                                  lam_h, lam_hu, lam_hv, lam_pitch, grad_n2, grad_rain_scale, dt,
+                                  t0 + k * dt, stream);
+            if (rc) return rc;
+        }
+    }
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
 
 int swe_ensemble_create(const swe_domain_desc* descs, int32_t n_members, swe_ensemble_t* out) {
     if (!descs || !out || n_members < 1) return fail(SWE_ERR_INVALID, "need at least one member descriptor");

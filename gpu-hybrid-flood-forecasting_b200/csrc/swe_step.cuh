@@ -58,6 +58,7 @@ struct DomainDev {
     const double* rain_t;  // hyetograph times (s), float64 copies of the float32 table
     const double* rain_r;  // rates (m/s)
     int n_rain;
+    double rain_scale;     // multiplies every rate (1 = the hyetograph as given)
 };
 
 struct StateView {
@@ -260,7 +261,7 @@ __device__ __forceinline__ FaceFlux face_flux(const Cell& lo, const Cell& hi, co
 // ---------------------------------------------------------------------------
 // np.interp(t, times, rates, left=default, right=default) in float64 with
 // separately rounded operations (shallow_water_2d.py:254-264).
-__device__ inline double rain_rate(const DomainDev& d, double t) {
+__device__ inline double rain_rate_unscaled(const DomainDev& d, double t) {
     const int n = d.n_rain;
     if (n <= 0) return d.default_rain;
     const double x0 = d.rain_t[0], xn = d.rain_t[n - 1];
@@ -282,6 +283,10 @@ __device__ inline double rain_rate(const DomainDev& d, double t) {
         if (v != v && yj == yj1) v = yj;
     }
     return v;
+}
+
+__device__ inline double rain_rate(const DomainDev& d, double t) {
+    return __dmul_rn(d.rain_scale, rain_rate_unscaled(d, t));
 }
 
 // Float32 scalars of a step of length dt starting at t.

@@ -37,6 +37,11 @@ EXPORTS = (
     "swe_set_timing",
     "swe_last_step_time",
     "swe_max_inverse_dt_noalloc",
+    "swe_domain_set_rain_scale",
+    "swe_domain_set_manning",
+    "swe_adjoint_step",
+    "swe_rollout_forward",
+    "swe_rollout_backward",
     "swe_ensemble_create",
     "swe_ensemble_destroy",
     "swe_ensemble_size",
@@ -120,6 +125,14 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_last_step_time": (ctypes.c_int, [_vp, ctypes.POINTER(_f64), ctypes.POINTER(_i64)]),
         "swe_max_inverse_dt_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _i32, _i32, _f64,
                                                       _f64, _f64, _f64, _vp, _vp]),
+        "swe_domain_set_rain_scale": (ctypes.c_int, [_vp, _f64]),
+        "swe_domain_set_manning": (ctypes.c_int, [_vp, _vp, _i32, _vp]),
+        "swe_adjoint_step": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp,
+                                            _i64, _vp, _vp, _f64, _f64, _vp]),
+        "swe_rollout_forward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _f64, _f64, _vp, _i32, _i32,
+                                               _vp, _vp, _i32, _vp]),
+        "swe_rollout_backward": (ctypes.c_int, [_vp, _vp, _i32, _i32, _f64, _f64, _vp, _i32, _i32, _vp, _vp,
+                                                _vp, _vp, _i64, _vp, _vp, _vp, _vp]),
         "swe_ensemble_create": (ctypes.c_int, [ctypes.POINTER(DomainDesc), _i32, ctypes.POINTER(_vp)]),
         "swe_ensemble_destroy": (ctypes.c_int, [_vp]),
         "swe_ensemble_size": (ctypes.c_int, [_vp]),

@@ -207,3 +207,36 @@ def street_depth(w: Workload, depth_m: float = 0.05) -> np.ndarray:
     x = (np.arange(cols, dtype=np.float64) + 0.5) * w.resolution_m
     plane = slope * (cols * w.resolution_m - x)[None, :]
     return np.where((w.bed - plane) < 1.0, depth_m, 0.0).astype(np.float32)
+
+
+def smoothed_lognormal_field(shape, *, median: float, sigma_log: float, seed: int,
+                             smooth_cells: int = 9) -> np.ndarray:
+    """Log-normal field (median, sigma of log) smoothed by a ``smooth_cells``-wide Gaussian."""
+    rng = np.random.default_rng(seed)
+    g = rng.normal(0.0, 1.0, shape)
+    radius = smooth_cells // 2
+    x = np.arange(-radius, radius + 1, dtype=np.float64)
+    sig = smooth_cells / 6.0
+    k = np.exp(-0.5 * (x / sig) ** 2)
+    k /= k.sum()
+    pad = np.pad(g, radius, mode="reflect")
+    sm = np.apply_along_axis(lambda v: np.convolve(v, k, mode="valid"), 1, pad)
+    sm = np.apply_along_axis(lambda v: np.convolve(v, k, mode="valid"), 0, sm)
+    sm /= sm.std() if sm.std() > 0 else 1.0
+    return (median * np.exp(sigma_log * sm)).astype(np.float32)
+
+
+def adjoint_case(rows: int = 512, cols: int = 512, *, dx: float = 2.0, truth_seed: int = 1,
+                 estimate_seed: int = 2, gauges: int = 16, gauge_seed: int = 7):
+    """The adjoint case: tilted-plane DEM as the 256x256 case (on a 512x512, dx = 2 m grid),
+    log-normal Manning n (median 0.03, sigma_log 0.3, 9-cell smoothing); the truth
+    uses ``truth_seed`` and the estimate ``estimate_seed``; ``gauges`` random gauge cells.
+    Returns (workload, n_truth, n_estimate, gauge_index)."""
+    w = tilted_bumps(rows, cols, dx=dx, seed=0)
+    n_truth = smoothed_lognormal_field((rows, cols), median=0.03, sigma_log=0.3, seed=truth_seed)
+    n_est = smoothed_lognormal_field((rows, cols), median=0.03, sigma_log=0.3, seed=estimate_seed)
+    rng = np.random.default_rng(gauge_seed)
+    idx = rng.choice(rows * cols, size=gauges, replace=False).astype(np.int64)
+    w.manning_n = n_est
+    w.name = f"adjoint_{rows}x{cols}"
+    return w, n_truth, n_est, idx

@@ -140,6 +140,46 @@ int swe_set_timing(swe_domain_t d, int32_t enable);
  * kernel of the last timed swe_run/swe_advance, and the step launches between. */
 int swe_last_step_time(swe_domain_t d, double *ms, int64_t *step_launches);
 
+/* Scale every rain rate of the hyetograph by `scale` (>= 0; 1 restores it).
+ * The differentiable rollout treats this scale as a parameter. */
+int swe_domain_set_rain_scale(swe_domain_t d, double scale);
+
+/* Replace the Manning n field (rows*cols contiguous, host or device); the
+ * domain mask is kept. */
+int swe_domain_set_manning(swe_domain_t d, const float *manning_n, int32_t on_host, void *stream);
+
+/* Reverse mode of one step (no counterpart in the reference, which never
+ * differentiates its solver): given lam = dL/dU_{k+1} and the state U_k that
+ * was stepped with (dt, time_s), write lam_out = dL/dU_k and ADD dL/d(n^2)
+ * into grad_n2 (rows*cols, device) and dL/d(rain scale) into *grad_rain_scale
+ * (one device double).  dt is held fixed (stop-gradient).  lam_out may alias lam. */
+int swe_adjoint_step(swe_domain_t d, const float *h, const float *hu, const float *hv, int64_t pitch,
+                     const float *lam_h, const float *lam_hu, const float *lam_hv, int64_t lam_pitch,
+                     float *lam_h_out, float *lam_hu_out, float *lam_hv_out, int64_t out_pitch,
+                     float *grad_n2, double *grad_rain_scale, double dt, double time_s, void *stream);
+
+/* Fixed-dt rollout with gauge observations: the forward of the differentiable
+ * rollout (no counterpart in the reference).  (h, hu, hv) advance IN PLACE by
+ * n_steps steps of dt from t0.  Every obs_every steps the depths at the
+ * n_gauges flat cell indices (device int64, row-major numbering) go to obs
+ * (device float32 [n_steps/obs_every][n_gauges]).  If ckpt is non-NULL the
+ * states at steps 0, ckpt_every, 2*ckpt_every, ... below n_steps are stored
+ * there as [k][3][rows][cols]. */
+int swe_rollout_forward(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, int32_t n_steps,
+                        double dt, double t0, const int64_t *gauge_index, int32_t n_gauges,
+                        int32_t obs_every, float *obs, float *ckpt, int32_t ckpt_every, void *stream);
+
+/* Reverse of swe_rollout_forward: from its checkpoints and dL/dobs (device,
+ * the layout of obs), writes dL/dU_0 to (lam_h, lam_hu, lam_hv), and ADDS
+ * dL/d(n^2) into grad_n2 and dL/d(rain scale) into *grad_rain_scale.  Each
+ * segment of ckpt_every steps is recomputed from its checkpoint into seg
+ * (device, ckpt_every*3*rows*cols floats) and reversed step by step. */
+int swe_rollout_backward(swe_domain_t d, const float *ckpt, int32_t ckpt_every, int32_t n_steps,
+                         double dt, double t0, const int64_t *gauge_index, int32_t n_gauges,
+                         int32_t obs_every, const float *grad_obs, float *lam_h, float *lam_hu,
+                         float *lam_hv, int64_t lam_pitch, float *grad_n2, double *grad_rain_scale,
+                         float *seg, void *stream);
+
 /* ---- Batched ensemble (no single counterpart in the reference: it batches many
  * reference runs -- NumpyShallowWaterSolver.run per member, numpy_solver/
  * shallow_water_2d.py:382-424 -- into one launch per step). ---- */
