@@ -69,6 +69,10 @@ def _args():
     ap.add_argument("--ensemble-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=2000)
+    ap.add_argument("--no-hybrid", action="store_true")
+    ap.add_argument("--hybrid-members", type=int, default=16)
+    ap.add_argument("--hybrid-size", type=int, default=1024)
+    ap.add_argument("--hybrid-intervals", type=int, default=10)
     return ap.parse_args()
 
 
@@ -271,6 +275,69 @@ def _adjoint(args, dev):
             "loss": float(loss), "grad_n_norm": float(n_t.grad.norm()), "grad_rain_scale": float(s_t.grad)}
 
 
+def _hybrid(args, dev):
+    """Coupled physics + corrector rollout: 16 urban 1024x1024 members, the
+    4-level (32/64/128/256) bfloat16 channels_last corrector on (h, hu, hv, z,
+    rain), a depth correction every 60 s at relaxation 0.5, 10 intervals."""
+    import torch
+
+    from hybrid_flood_b200.ensemble import B200Ensemble
+    from hybrid_flood_b200.hybrid import HybridInputs, run_coupled_ensemble
+    from hybrid_flood_b200.unet import corrector_4level
+    from hybrid_flood_b200.workloads import as_member, street_depth, urban
+
+    torch.backends.cudnn.benchmark = True
+    M, S = args.hybrid_members, args.hybrid_size
+    ws = [urban(S, S, seed=2000 + m, rain_scale=float(np.exp(0.4 * np.random.default_rng(m).normal())))
+          for m in range(M)]
+    ens = B200Ensemble([as_member(w) for w in ws], arithmetic=args.arith, device=dev)
+    depths = [street_depth(w) for w in ws]
+    states = [tuple(t.cpu().numpy() for t in s) for s in ens.initial_states(depths)]
+    z = np.stack([w.bed for w in ws])
+    h0 = np.stack([s[0] for s in states])
+    hi = HybridInputs(None, None,
+                      np.array([h0.mean(), 0.0, 0.0, z.mean(), 5.0], np.float32),
+                      np.array([max(h0.std(), 1e-3), 0.05, 0.05, max(z.std(), 1e-3), 5.0], np.float32),
+                      25.0, np.array([0.01], np.float32))
+    torch.manual_seed(0)
+    net = corrector_4level()
+    with torch.no_grad():
+        net.residual_head.weight.normal_(0.0, 0.01)
+    net = net.to(device=dev, dtype=torch.bfloat16, memory_format=torch.channels_last).eval()
+    kw = dict(max_substeps_per_interval=5000, correction_relaxation=0.5, feature_layout="state5", keep_states=False)
+    run_coupled_ensemble(ens, states, net, hi, np.array([0.0, 60.0]), **kw)  # warm-up: graphs, cuDNN plans
+    times = 60.0 * np.arange(args.hybrid_intervals + 1)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    traj, steps = run_coupled_ensemble(ens, states, net, hi, times, **kw)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    total_ms = e0.elapsed_time(e1)
+    # the corrector alone on the same batch, for the time split
+    feats = torch.zeros((M, S, S, 5), dtype=torch.bfloat16, device=dev).permute(0, 3, 1, 2)
+    with torch.no_grad():
+        net(feats)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(3):
+            net(feats)
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    net_ms = e0.elapsed_time(e1) / 3
+    cells = M * S * S
+    phys_updates = float(S * S * steps.sum())
+    finite = all(bool(torch.isfinite(t).all()) for tr in traj for t in tr)
+    return {"workload": f"{M} urban {S}x{S} members dx=1m, correction every 60 s, relaxation 0.5, "
+                        f"{args.hybrid_intervals} intervals, 4-level bf16 channels_last corrector (5 in, 1 out)",
+            "members": M, "cells": cells, "intervals": args.hybrid_intervals, "total_ms": total_ms,
+            "ms_per_interval": total_ms / args.hybrid_intervals, "physics_steps_mean": float(steps.mean()),
+            "physics_steps_max": int(steps.max()), "corrector_ms_per_interval": net_ms,
+            "corrector_share": net_ms * args.hybrid_intervals / total_ms,
+            "cell_updates_per_s": phys_updates / (total_ms / 1e3), "finite": finite}
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
@@ -378,6 +445,9 @@ def run_b200(args, rank: int, world: int):
     adj = None
     if not args.no_adjoint and rank == 0:
         adj = _adjoint(args, dev)
+    hyb = None
+    if not args.no_hybrid and rank == 0:
+        hyb = _hybrid(args, dev)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -409,6 +479,8 @@ def run_b200(args, rank: int, world: int):
         line["ensemble"] = ens
     if adj:
         line["adjoint"] = adj
+    if hyb:
+        line["hybrid"] = hyb
     if not args.no_cpu_baseline:
         from oracle import cport
 

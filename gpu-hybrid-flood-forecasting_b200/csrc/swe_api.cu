@@ -20,6 +20,7 @@
 #include "swe_step.cuh"
 #include "swe_step_pair.cuh"
 #include "swe_adjoint.cuh"
+#include "swe_hybrid.cuh"
 
 using namespace swe;
 
@@ -109,6 +110,10 @@ struct swe_domain {
     int occ_cache[2][2] = {{0, 0}, {0, 0}};  // [V-1][run]: CTAs per SM of the step kernels
     float* lupd[3] = {nullptr, nullptr, nullptr};  // adjoint scratch
     int64_t lpitch = 0;
+    double* times64_dev = nullptr;  // float64 targets of advance_to
+    double* corr_sums = nullptr;    // volume sums of the residual correction
+    float* corr_prov = nullptr;     // provisional-depth plane of the correction
+    unsigned* done_counter = nullptr;  // set by an ensemble: shared completion counter
 };
 
 namespace {
@@ -256,7 +261,8 @@ int copy_plane(float* dst, int64_t dpitch, const float* src, int64_t spitch, int
 // clock, the first CFL dt and volume0.  Shared by swe_run, swe_advance and the
 // ensemble.
 int begin_run(swe_domain* d, StateView init, const float* times_host, int n_times, double t_start,
-              int n_out, int max_steps, float* out_h, float* out_hu, float* out_hv, cudaStream_t st) {
+              int n_out, int max_steps, float* out_h, float* out_hu, float* out_hv, cudaStream_t st,
+              const double* times64_host = nullptr) {
     const int rows = d->dd.rows, cols = d->dd.cols;
     int rc = ensure_ping(d);
     if (rc) return rc;
@@ -275,6 +281,12 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
     }
     SWE_CK(cudaMemcpyAsync(d->times_dev, times_host, sizeof(float) * (size_t)n_times,
                            cudaMemcpyHostToDevice, st));
+    if (times64_host) {
+        if (n_times > 2) return fail(SWE_ERR_INVALID, "float64 targets support one interval");
+        if (!d->times64_dev) SWE_CK(cudaMalloc(&d->times64_dev, 2 * sizeof(double)));
+        SWE_CK(cudaMemcpyAsync(d->times64_dev, times64_host, sizeof(double) * (size_t)n_times,
+                               cudaMemcpyHostToDevice, st));
+    }
     if (out_h) {
         float* outs[3] = {out_h, out_hu, out_hv};
         for (int f = 0; f < 3; ++f) {
@@ -289,11 +301,14 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
     c0.max_steps = max_steps;
     c0.t_start = t_start;
     c0.times = d->times_dev;
+    c0.times64 = times64_host ? d->times64_dev : nullptr;
+    c0.done_counter = d->done_counter;
     c0.out_h = out_h;
     c0.out_hu = out_hu;
     c0.out_hv = out_hv;
     c0.out_plane = (int64_t)rows * cols;
     c0.snap = -1;
+    c0.reach = -1;
     // Pageable source: the copy is staged before cudaMemcpyAsync returns.
     SWE_CK(cudaMemcpyAsync(d->ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, st));
     StateView v0{d->ping[0][0], d->ping[0][1], d->ping[0][2], d->ppitch};
@@ -305,13 +320,15 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
 // Shared run driver for swe_run and swe_advance.
 int run_driver(swe_domain* d, StateView init, const float* times_host, int n_times,
                double t_start, int n_out, int max_steps, float* out_h, float* out_hu,
-               float* out_hv, swe_run_result* res, cudaStream_t st, int* final_buf) {
+               float* out_hv, swe_run_result* res, cudaStream_t st, int* final_buf,
+               const double* times64_host = nullptr) {
     int rc = ensure_ping(d);
     if (rc) return rc;
     const Plan pl = make_plan(d, d->run_vec, true);
     rc = ensure_parts(d, std::max(pl.blocks, reduce_blocks(d)));
     if (rc) return rc;
-    rc = begin_run(d, init, times_host, n_times, t_start, n_out, max_steps, out_h, out_hu, out_hv, st);
+    rc = begin_run(d, init, times_host, n_times, t_start, n_out, max_steps, out_h, out_hu, out_hv, st,
+                   times64_host);
     if (rc) return rc;
     int64_t launched = 0;
     d->launches = 1;
@@ -380,6 +397,9 @@ void free_domain(swe_domain* d) {
         for (int f = 0; f < 3; ++f) cudaFree(d->ping[b][f]);
     cudaFree(d->times_dev);
     for (int q = 0; q < 3; ++q) cudaFree(d->lupd[q]);
+    cudaFree(d->times64_dev);
+    cudaFree(d->corr_sums);
+    cudaFree(d->corr_prov);
     for (int i = 0; i < 2; ++i) {
         if (d->poll_ev[i]) cudaEventDestroy(d->poll_ev[i]);
         if (d->time_ev[i]) cudaEventDestroy(d->time_ev[i]);
@@ -432,6 +452,9 @@ struct swe_ensemble {
     bool timed_valid = false;
     int64_t timed_steps = 0;
     int64_t launches = 0;
+    unsigned* done_counter = nullptr;       // device: members finished in advance_to
+    unsigned* done_host = nullptr;          // pinned: two polled copies of it
+    cudaEvent_t poll_ev[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -533,6 +556,42 @@ int ens_graph(swe_ensemble* e, int K) {
     return SWE_OK;
 }
 
+// Reads every member's Control block, fills its run result and copies its
+// final planes to the caller's buffers.  Error statuses: any member's, the
+// first one met; a member short of its target counts only when need_target.
+int ens_collect(swe_ensemble* e, float* const* h, float* const* hu, float* const* hv, const int64_t* pitch,
+                swe_run_result* results, cudaStream_t st, bool need_target) {
+    const int n = (int)e->doms.size();
+    SWE_CK(cudaStreamSynchronize(st));
+    int status = SWE_OK;
+    for (int m = 0; m < n; ++m) {
+        swe_domain* d = e->doms[m];
+        SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
+        const Control& c = d->ctl_host[0];
+        swe_run_result& r = results[m];
+        r.final_time_s = c.t;
+        r.outputs_written = c.idx;
+        r.steps_used = c.steps;
+        r.status = c.status;
+        r.reserved = 0;
+        for (int i = 0; i < 6; ++i) r.ledger[i] = c.ledger[i];
+        if (c.status && !status) status = c.status;
+        if (need_target && !c.done && !status) status = SWE_ERR_MAX_STEPS;
+        float* outs[3] = {h[m], hu[m], hv[m]};
+        const int fb = c.steps & 1;
+        for (int f = 0; f < 3; ++f) {
+            const int rc = copy_plane(outs[f], pitch[m], d->ping[fb][f], d->ppitch, d->dd.rows, d->dd.cols, st);
+            if (rc) return rc;
+        }
+    }
+    SWE_CK(cudaStreamSynchronize(st));
+    if (status == SWE_ERR_NONFINITE) return fail(SWE_ERR_NONFINITE, "non-finite values reached a member's CFL reduction");
+    if (status == SWE_ERR_MAX_STEPS) return fail(status, "an ensemble member did not reach its target time");
+    if (status) return fail(status, "an ensemble member stopped with an error status");
+    return SWE_OK;
+}
+
+
 void free_ensemble(swe_ensemble* e) {
     if (!e) return;
     for (auto* d : e->doms) free_domain(d);
@@ -540,8 +599,12 @@ void free_ensemble(swe_ensemble* e) {
     cudaFree(e->items_dev);
     if (e->graph) cudaGraphExecDestroy(e->graph);
     if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 2; ++i) {
         if (e->time_ev[i]) cudaEventDestroy(e->time_ev[i]);
+        if (e->poll_ev[i]) cudaEventDestroy(e->poll_ev[i]);
+    }
+    cudaFree(e->done_counter);
+    cudaFreeHost(e->done_host);
     delete e;
 }
 
@@ -956,6 +1019,7 @@ int swe_max_inverse_dt(swe_domain_t d, const float* h, const float* hu, const fl
     Control c0;
     std::memset(&c0, 0, sizeof(c0));
     c0.snap = -1;
+    c0.reach = -1;
     SWE_CK(cudaMemcpyAsync(d->ctl_scratch, &c0, sizeof(Control), cudaMemcpyHostToDevice, st));
     launch_reduce(d, StateView{h, hu, hv, pitch}, d->ctl_scratch, st);
     SWE_CK(cudaGetLastError());
@@ -1036,6 +1100,119 @@ int swe_advance(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, i
 }
 
 int64_t swe_last_launch_count(swe_domain_t d) { return d ? d->launches : -1; }
+
+int swe_advance_to(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, double t_start,
+                   double t_target, int32_t max_steps, swe_run_result* result, void* stream) {
+    if (!d || !result) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    if (!(t_target >= t_start) || max_steps < 0) return fail(SWE_ERR_INVALID, "need t_target >= t_start and max_steps >= 0");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float times[2] = {(float)t_start, (float)t_target};
+    const double times64[2] = {t_start, t_target};
+    int fb = 0;
+    rc = run_driver(d, StateView{h, hu, hv, pitch}, times, 2, t_start, 2, max_steps, nullptr, nullptr, nullptr,
+                    result, st, &fb, times64);
+    if (rc) return rc;
+    float* outs[3] = {h, hu, hv};
+    for (int f = 0; f < 3; ++f) {
+        rc = copy_plane(outs[f], pitch, d->ping[fb][f], d->ppitch, d->dd.rows, d->dd.cols, st);
+        if (rc) return rc;
+    }
+    SWE_CK(cudaStreamSynchronize(st));
+    if (result->status == SWE_ERR_NONFINITE) return fail(SWE_ERR_NONFINITE, "non-finite values reached the CFL reduction");
+    if (result->status == SWE_ERR_MAX_STEPS) {
+        char msg[160];
+        std::snprintf(msg, sizeof msg, "max_steps=%d did not reach t=%.6f s (stopped at %.6f s)", max_steps,
+                      t_target, result->final_time_s);
+        return fail(SWE_ERR_MAX_STEPS, msg);
+    }
+    return SWE_OK;
+}
+
+int swe_network_features(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch,
+                         int32_t layout, const float* mean, const float* stddev, float rain_feature,
+                         const float* terrain, const float* roughness, void* out, int32_t out_bf16,
+                         void* stream) {
+    if (!d || !out || !mean || !stddev) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    if (layout != kFeatRef6 && layout != kFeatState5) return fail(SWE_ERR_INVALID, "unknown feature layout");
+    FeatureArgs a{};
+    a.rows = d->dd.rows;
+    a.cols = d->dd.cols;
+    a.s = StateView{h, hu, hv, pitch};
+    a.nm = d->nm;
+    a.bed = d->bed;
+    a.spitch = d->dd.spitch;
+    a.terrain = terrain;
+    a.roughness = roughness;
+    const int nstat = layout == kFeatRef6 ? 3 : 5;
+    for (int q = 0; q < 5; ++q) {
+        a.mean[q] = q < nstat ? mean[q] : 0.f;
+        const float sd = q < nstat ? stddev[q] : 1.f;
+        if (!(sd > 0.f)) return fail(SWE_ERR_INVALID, "standard deviations must be positive");
+        a.stdv[q] = sd;
+    }
+    a.rain_feature = rain_feature;
+    a.dry = d->dd.k.dry;
+    a.layout = layout;
+    a.channels = layout == kFeatRef6 ? 6 : 5;
+    a.out = out;
+    a.out_bf16 = out_bf16 ? 1 : 0;
+    const int64_t n = (int64_t)a.rows * a.cols;
+    features_kernel<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)d->sms * 8), 256, 0,
+                      static_cast<cudaStream_t>(stream)>>>(a);
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
+int swe_apply_correction(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch,
+                         const void* residual, int32_t residual_bf16, int64_t res_stride_row,
+                         int64_t res_stride_col, int64_t res_stride_channel, int32_t res_channels,
+                         const float* clip_limits, double relaxation, float* h_out, float* hu_out,
+                         float* hv_out, int64_t out_pitch, void* stream) {
+    if (!d || !residual) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    rc = check_state_ptrs(h_out, hu_out, hv_out, out_pitch, d->dd.cols);
+    if (rc) return rc;
+    if (res_channels != 1 && res_channels != 3) return fail(SWE_ERR_INVALID, "residual must have 1 or 3 channels");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!d->corr_sums) SWE_CK(cudaMalloc(&d->corr_sums, 2 * sizeof(double)));
+    if (!d->corr_prov) SWE_CK(cudaMalloc(&d->corr_prov, sizeof(float) * (size_t)d->dd.spitch * d->dd.rows));
+    SWE_CK(cudaMemsetAsync(d->corr_sums, 0, 2 * sizeof(double), st));
+    CorrectionArgs a{};
+    a.rows = d->dd.rows;
+    a.cols = d->dd.cols;
+    a.s = StateView{h, hu, hv, pitch};
+    a.out = StateOut{h_out, hu_out, hv_out, out_pitch};
+    a.prov = d->corr_prov;
+    a.prov_pitch = d->dd.spitch;
+    a.nm = d->nm;
+    a.spitch = d->dd.spitch;
+    a.res = residual;
+    a.rs_r = res_stride_row;
+    a.rs_c = res_stride_col;
+    a.rs_ch = res_stride_channel;
+    a.res_channels = res_channels;
+    a.res_bf16 = residual_bf16 ? 1 : 0;
+    for (int q = 0; q < 3; ++q) {
+        a.lim[q] = (clip_limits && q < res_channels) ? clip_limits[q] : INFINITY;
+        if (!(a.lim[q] >= 0.f)) return fail(SWE_ERR_INVALID, "clip limits must be >= 0");
+    }
+    a.relax = (float)relaxation;
+    a.dry = d->dd.k.dry;
+    a.eps = 1.1920929e-07f;  // float32 machine epsilon (jnp.finfo(float32).eps)
+    a.sums = d->corr_sums;
+    const int64_t n = (int64_t)a.rows * a.cols;
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)d->sms * 8);
+    correction_sums_kernel<<<blocks, 256, 0, st>>>(a);
+    correction_apply_kernel<<<blocks, 256, 0, st>>>(a);
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
 
 int swe_rollout_forward(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, int32_t n_steps,
                         double dt, double t0, const int64_t* gauge_index, int32_t n_gauges,
@@ -1218,30 +1395,77 @@ int swe_ensemble_advance(swe_ensemble_t e, float* const* h, float* const* hu, fl
         e->timed_steps = n_steps;
         e->timed_valid = true;
     }
-    SWE_CK(cudaStreamSynchronize(st));
-    int status = SWE_OK;
+    return ens_collect(e, h, hu, hv, pitch, results, st, false);
+}
+
+int swe_ensemble_advance_to(swe_ensemble_t e, float* const* h, float* const* hu, float* const* hv,
+                            const int64_t* pitch, const double* start_s, double target_s, int32_t max_steps,
+                            swe_run_result* results, void* stream) {
+    if (!e || !h || !hu || !hv || !pitch || !results || !start_s) return fail(SWE_ERR_INVALID, "null argument");
+    if (max_steps < 0) return fail(SWE_ERR_INVALID, "max_steps must be >= 0");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int n = (int)e->doms.size();
+    if (!e->done_counter) {
+        SWE_CK(cudaMalloc(&e->done_counter, sizeof(unsigned)));
+        SWE_CK(cudaHostAlloc(&e->done_host, 2 * sizeof(unsigned), cudaHostAllocDefault));
+        SWE_CK(cudaEventCreateWithFlags(&e->poll_ev[0], cudaEventDisableTiming));
+        SWE_CK(cudaEventCreateWithFlags(&e->poll_ev[1], cudaEventDisableTiming));
+    }
+    SWE_CK(cudaMemsetAsync(e->done_counter, 0, sizeof(unsigned), st));
     for (int m = 0; m < n; ++m) {
         swe_domain* d = e->doms[m];
-        SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
-        const Control& c = d->ctl_host[0];
-        swe_run_result& r = results[m];
-        r.final_time_s = c.t;
-        r.outputs_written = c.idx;
-        r.steps_used = c.steps;
-        r.status = c.status;
-        r.reserved = 0;
-        for (int i = 0; i < 6; ++i) r.ledger[i] = c.ledger[i];
-        if (c.status) status = c.status;
-        float* outs[3] = {h[m], hu[m], hv[m]};
-        const int fb = c.steps & 1;
-        for (int f = 0; f < 3; ++f) {
-            const int rc = copy_plane(outs[f], pitch[m], d->ping[fb][f], d->ppitch, d->dd.rows, d->dd.cols, st);
-            if (rc) return rc;
+        int rc = check_state_ptrs(h[m], hu[m], hv[m], pitch[m], d->dd.cols);
+        if (rc) return rc;
+        if (!(target_s >= start_s[m])) return fail(SWE_ERR_INVALID, "every start time must be <= the target");
+        const float times[2] = {(float)start_s[m], (float)target_s};
+        const double times64[2] = {start_s[m], target_s};
+        d->done_counter = e->done_counter;
+        rc = begin_run(d, StateView{h[m], hu[m], hv[m], pitch[m]}, times, 2, start_s[m], 2, max_steps, nullptr,
+                       nullptr, nullptr, st, times64);
+        d->done_counter = nullptr;
+        if (rc) return rc;
+    }
+    // K-step graphs until every member is done.  The counter is read one
+    // graph late so the host never waits on the graph just queued.
+    const int K = 50;
+    e->timed_valid = false;
+    if (e->timing) {
+        if (!e->time_ev[0]) {
+            SWE_CK(cudaEventCreate(&e->time_ev[0]));
+            SWE_CK(cudaEventCreate(&e->time_ev[1]));
+        }
+        SWE_CK(cudaEventRecord(e->time_ev[0], st));
+    }
+    int rc = ens_graph(e, K);
+    if (rc) return rc;
+    const int64_t max_graphs = ((int64_t)max_steps + K - 1) / K;
+    int64_t g = 0;
+    e->done_host[0] = e->done_host[1] = 0;
+    for (; g < max_graphs; ++g) {
+        SWE_CK(cudaGraphLaunch(e->graph, st));
+        SWE_CK(cudaMemcpyAsync(&e->done_host[g & 1], e->done_counter, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        SWE_CK(cudaEventRecord(e->poll_ev[g & 1], st));
+        if (g > 0) {
+            SWE_CK(cudaEventSynchronize(e->poll_ev[(g - 1) & 1]));
+            if (e->done_host[(g - 1) & 1] >= (unsigned)n) {
+                ++g;
+                break;
+            }
         }
     }
-    SWE_CK(cudaStreamSynchronize(st));
-    if (status == SWE_ERR_NONFINITE) return fail(SWE_ERR_NONFINITE, "non-finite values reached a member's CFL reduction");
-    if (status) return fail(status, "an ensemble member stopped with an error status");
+    e->launches = n + g * K;
+    if (e->timing) {
+        SWE_CK(cudaEventRecord(e->time_ev[1], st));
+        e->timed_steps = g * K;
+        e->timed_valid = true;
+    }
+    return ens_collect(e, h, hu, hv, pitch, results, st, true);
+}
+
+int swe_ensemble_member(swe_ensemble_t e, int32_t m, swe_domain_t* out) {
+    if (!e || !out) return fail(SWE_ERR_INVALID, "null argument");
+    if (m < 0 || m >= (int)e->doms.size()) return fail(SWE_ERR_INVALID, "member index out of range");
+    *out = e->doms[m];
     return SWE_OK;
 }
 

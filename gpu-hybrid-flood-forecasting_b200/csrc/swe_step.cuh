@@ -81,6 +81,7 @@ struct Control {
     double dt;         // dt of the next step (already limited by the output target)
     StepScalars s;     // float32 scalars of the next step
     int snap;          // output index written by the next step, -1 if none
+    int reach;         // output time reached by the next step (recorded or not), -1 if none
     int idx;           // next output index to fill
     int steps;         // steps taken
     int done;          // nonzero: all outputs written, step cap hit or failure
@@ -90,6 +91,8 @@ struct Control {
     int n_out, max_steps;
     double t_start;               // clock value set by the init reduction
     const float* times;           // device copy of the float32 output times
+    const double* times64;        // float64 targets instead of `times` (advance_to), or null
+    unsigned* done_counter;       // incremented once when this run finishes (ensembles), or null
     float* out_h;                 // n_out x rows x cols snapshots (may be null)
     float* out_hu;
     float* out_hv;
@@ -313,26 +316,26 @@ __device__ inline double cfl_dt_from(const DomainDev& d, float maxinv) {
 // new time reaches target - 1e-7, stop when all outputs are written or the step
 // cap is reached.
 __device__ inline void plan_next(const DomainDev& d, Control& c) {
+    c.snap = -1;
+    c.reach = -1;
     if (c.idx >= c.n_out || c.steps >= c.max_steps) {
         c.done = 1;
-        c.snap = -1;
         return;
     }
     if (!(c.maxinv == c.maxinv) || isinf(c.maxinv)) {
         c.done = 1;
         c.status = 4;  // SWE_ERR_NONFINITE
-        c.snap = -1;
         return;
     }
-    const double target = (double)c.times[c.idx];
+    const double target = c.times64 ? c.times64[c.idx] : (double)c.times[c.idx];
     double dt = cfl_dt_from(d, c.maxinv);
     const double remain = __dsub_rn(target, c.t);
     if (remain < dt) dt = remain;
     c.dt = dt;
     c.s = step_scalars(d, dt, c.t);
-    c.snap = (__dadd_rn(c.t, dt) >= __dsub_rn(target, 1.0e-7)) ? c.idx : -1;
-    // Without output buffers (fixed-count advance) nothing is recorded.
-    if (c.out_h == nullptr) c.snap = -1;
+    c.reach = (__dadd_rn(c.t, dt) >= __dsub_rn(target, 1.0e-7)) ? c.idx : -1;
+    // Without output buffers (advance, advance_to) nothing is recorded.
+    c.snap = c.out_h ? c.reach : -1;
 }
 
 template <typename T>
@@ -474,7 +477,7 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     } else {
         c.t = __dadd_rn(c.t, c.dt);
         c.steps += 1;
-        if (c.snap >= 0) c.idx = c.snap + 1;
+        if (c.reach >= 0) c.idx = c.reach + 1;
         c.ledger[1] = vol * area;
         c.ledger[2] += rain * area;
         c.ledger[3] += outflow;
@@ -488,7 +491,9 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
         c.status = 6;  // SWE_ERR_TIMEOUT
         c.done = 1;
         c.snap = -1;
+        c.reach = -1;
     }
+    if (c.done && c.done_counter) atomicAdd(c.done_counter, 1u);
     *ctl = c;
     __threadfence();
 }

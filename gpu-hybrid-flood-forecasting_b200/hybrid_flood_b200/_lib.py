@@ -42,11 +42,16 @@ EXPORTS = (
     "swe_adjoint_step",
     "swe_rollout_forward",
     "swe_rollout_backward",
+    "swe_advance_to",
+    "swe_network_features",
+    "swe_apply_correction",
     "swe_ensemble_create",
     "swe_ensemble_destroy",
     "swe_ensemble_size",
     "swe_ensemble_set_rows_per_warp",
     "swe_ensemble_advance",
+    "swe_ensemble_advance_to",
+    "swe_ensemble_member",
     "swe_ensemble_set_timing",
     "swe_ensemble_last_step_time",
     "swe_ensemble_last_launch_count",
@@ -133,12 +138,21 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
                                                _vp, _vp, _i32, _vp]),
         "swe_rollout_backward": (ctypes.c_int, [_vp, _vp, _i32, _i32, _f64, _f64, _vp, _i32, _i32, _vp, _vp,
                                                 _vp, _vp, _i64, _vp, _vp, _vp, _vp]),
+        "swe_advance_to": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _f64, _f64, _i32, ctypes.POINTER(RunResult),
+                                          _vp]),
+        "swe_network_features": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _vp, _vp, ctypes.c_float, _vp,
+                                                _vp, _vp, _i32, _vp]),
+        "swe_apply_correction": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _vp, _i32, _i64, _i64, _i64, _i32,
+                                                _vp, _f64, _vp, _vp, _vp, _i64, _vp]),
         "swe_ensemble_create": (ctypes.c_int, [ctypes.POINTER(DomainDesc), _i32, ctypes.POINTER(_vp)]),
         "swe_ensemble_destroy": (ctypes.c_int, [_vp]),
         "swe_ensemble_size": (ctypes.c_int, [_vp]),
         "swe_ensemble_set_rows_per_warp": (ctypes.c_int, [_vp, _i32]),
         "swe_ensemble_advance": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp,
                                                 ctypes.POINTER(RunResult), _vp]),
+        "swe_ensemble_advance_to": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f64, _i32,
+                                                   ctypes.POINTER(RunResult), _vp]),
+        "swe_ensemble_member": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_vp)]),
         "swe_ensemble_set_timing": (ctypes.c_int, [_vp, _i32]),
         "swe_ensemble_last_step_time": (ctypes.c_int, [_vp, ctypes.POINTER(_f64), ctypes.POINTER(_i64)]),
         "swe_ensemble_last_launch_count": (ctypes.c_int64, [_vp]),

@@ -88,6 +88,7 @@ class B200Ensemble:
         self.masks = [torch.from_numpy(np.asarray(m["domain_mask"], dtype=bool)).to(self.device) for m in members]
         self.arithmetic = arithmetic
         self.rows_per_warp = 16
+        self.dry_tolerances = [float(m.get("dry_tolerance_m", 1.0e-4)) for m in members]
 
     def __del__(self):
         h = getattr(self, "_handle", None)
@@ -141,6 +142,40 @@ class B200Ensemble:
                                                 starts, res, _stream(self.device))
         _lib.check(rc, "swe_ensemble_advance")
         return [(float(r.final_time_s), int(r.steps_used), dict(zip(LEDGER_KEYS, list(r.ledger)))) for r in res]
+
+    def advance_to_(self, states: list[SWEState], start_times, target_time_s: float,
+                    max_steps: int) -> list[tuple]:
+        """Advance every member IN PLACE from its start time to ``target_time_s``.
+
+        At most ``max_steps`` CFL-limited steps per member; 50-step graphs are
+        replayed until every member is done.  Returns one
+        ``(final_time_s, steps_used, ledger)`` per member; a member stopped
+        short by the cap reports where it stopped.
+        """
+        n = len(self.shapes)
+        if len(states) != n:
+            raise ValueError(f"expected {n} states, got {len(states)}")
+        self._check_states(states)
+        starts = [float(start_times)] * n if np.isscalar(start_times) else [float(t) for t in start_times]
+        arr = lambda typ, vals: (typ * n)(*vals)  # noqa: E731
+        res = (_lib.RunResult * n)()
+        with torch.cuda.device(self.device):
+            rc = self._lib.swe_ensemble_advance_to(
+                self._handle, arr(ctypes.c_void_p, [s.h.data_ptr() for s in states]),
+                arr(ctypes.c_void_p, [s.hu.data_ptr() for s in states]),
+                arr(ctypes.c_void_p, [s.hv.data_ptr() for s in states]),
+                arr(ctypes.c_int64, [int(s.h.stride(0)) for s in states]), arr(ctypes.c_double, starts),
+                float(target_time_s), int(max_steps), res, _stream(self.device))
+        if rc != _lib.SWE_ERR_MAX_STEPS:
+            _lib.check(rc, "swe_ensemble_advance_to")
+        return [(float(r.final_time_s), int(r.steps_used), dict(zip(LEDGER_KEYS, list(r.ledger)))) for r in res]
+
+    def _check_states(self, states) -> None:
+        for st, shape in zip(states, self.shapes):
+            for t in st:
+                if not (isinstance(t, torch.Tensor) and t.device == self.device and t.dtype == torch.float32
+                        and tuple(t.shape) == shape and t.stride(-1) == 1):
+                    raise ValueError("ensemble states must be device float32 [rows, cols] tensors per member")
 
     def set_rows_per_warp(self, rows: int) -> None:
         with torch.cuda.device(self.device):

@@ -287,6 +287,30 @@ class B200ShallowWaterSolver:
         _lib.check(rc, "advance")
         return float(res.final_time_s), int(res.steps_used), dict(zip(LEDGER_KEYS, list(res.ledger)))
 
+    def advance_to_(self, state: SWEState, start_time_s: float, target_time_s: float,
+                    max_steps: int) -> tuple[float, int, dict]:
+        """Advance ``state`` IN PLACE from ``start_time_s`` to ``target_time_s``.
+
+        CFL-limited steps with ``dt = min(cfl_dt, target - t)``, at most
+        ``max_steps`` of them (``advance_physics_to_time``,
+        ``src/hybrid_flood/hybrid/coupled_forecast.py:123-161``).  Returns
+        ``(final_time_s, steps_used, ledger)``; when the step cap stops the run
+        short, ``final_time_s`` is where it stopped and the state is the one
+        reached there.
+        """
+        res = _lib.RunResult()
+        for t in state:
+            if not (isinstance(t, torch.Tensor) and t.device == self.device and t.dtype == torch.float32
+                    and tuple(t.shape) == self.shape and t.stride(-1) == 1):
+                raise ValueError("advance_to_ needs device float32 [rows, cols] tensors")
+        with torch.cuda.device(self.device):
+            rc = self._lib.swe_advance_to(self._handle, _ptr(state.h), _ptr(state.hu), _ptr(state.hv),
+                                          _pitch(state.h), float(start_time_s), float(target_time_s),
+                                          int(max_steps), ctypes.byref(res), _stream(self.device))
+        if rc != _lib.SWE_ERR_MAX_STEPS:
+            _lib.check(rc, "advance_to")
+        return float(res.final_time_s), int(res.steps_used), dict(zip(LEDGER_KEYS, list(res.ledger)))
+
     def advance(self, state, n_steps: int, start_time_s: float = 0.0):
         """Functional form of :meth:`advance_`: returns ``(new_state, final_time_s, steps_used, ledger)``."""
         st = _as_state(state, self.device, self.shape)

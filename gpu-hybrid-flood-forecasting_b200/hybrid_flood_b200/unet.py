@@ -1,0 +1,118 @@
+"""Residual U-Net corrector of the hybrid rollout.
+
+Layer plan of ``TorchResidualUNet``
+(``src/hybrid_flood/benchmark/pytorch_residual_net.py:79-170``, the PyTorch
+twin of the Flax ``ml/residual_net.py:43-111``): per level two k×k
+convolutions with an activation each; a 2×2 stride-2 convolution (TF ``SAME``
+padding) into the next level's width; on the way up a 2×2 stride-2 transposed
+convolution, the skip concatenated after it, and two convolutions; a zero-
+initialised 1×1 head.  Submodule names equal the reference's so its
+``state_dict`` loads unchanged.
+
+On the B200 the network runs in bfloat16 with ``channels_last`` tensors (NHWC
+in memory): the feature kernel writes NHWC bfloat16 directly and the correction
+kernel reads the bfloat16 NHWC residual in place, so the hand-off around the
+convolutions (cuDNN, tensor cores) needs no layout or dtype conversion.
+"""
+
+from __future__ import annotations
+
+from collections.abc import Sequence
+
+import torch
+import torch.nn.functional as F
+from torch import nn
+
+_ACTIVATIONS = {
+    "relu": lambda: nn.ReLU(),
+    "gelu": lambda: nn.GELU(approximate="tanh"),  # Flax's default GELU is the tanh form
+    "silu": lambda: nn.SiLU(),
+    "tanh": lambda: nn.Tanh(),
+}
+
+
+def make_activation(name: str) -> nn.Module:
+    key = name.lower()
+    if key not in _ACTIVATIONS:
+        raise ValueError(f"Unsupported activation {name!r}; choose one of {sorted(_ACTIVATIONS)}.")
+    return _ACTIVATIONS[key]()
+
+
+class ConvPair(nn.Module):
+    """Two same-size k×k convolutions, each followed by the activation."""
+
+    def __init__(self, cin: int, cout: int, k: int, activation: str) -> None:
+        super().__init__()
+        self.conv_1 = nn.Conv2d(cin, cout, k, padding=k // 2)
+        self.activation_1 = make_activation(activation)
+        self.conv_2 = nn.Conv2d(cout, cout, k, padding=k // 2)
+        self.activation_2 = make_activation(activation)
+
+    def forward(self, x: torch.Tensor) -> torch.Tensor:
+        return self.activation_2(self.conv_2(self.activation_1(self.conv_1(x))))
+
+
+def pad_same_stride2(x: torch.Tensor) -> torch.Tensor:
+    """TF/Flax ``SAME`` padding of a 2×2 stride-2 window: an odd extent gets one
+    trailing row/column, an even one none."""
+    ph, pw = x.shape[-2] % 2, x.shape[-1] % 2
+    return F.pad(x, (0, pw, 0, ph)) if (ph or pw) else x
+
+
+class ResidualUNet(nn.Module):
+    """U-Net residual corrector; NCHW in and out (``channels_last`` memory preferred)."""
+
+    def __init__(self, *, input_channels: int, depth: int, channels: Sequence[int], activation: str = "relu",
+                 kernel_size: int = 3, output_channels: int = 3) -> None:
+        super().__init__()
+        if depth < 1:
+            raise ValueError("U-Net depth must be positive.")
+        if len(channels) < depth:
+            raise ValueError("The channel list must contain at least one value per U-Net depth.")
+        if kernel_size < 1 or kernel_size % 2 == 0:
+            raise ValueError("The convolution kernel size must be a positive odd integer.")
+        widths = [int(c) for c in channels[:depth]]
+        self.widths = tuple(widths)
+        self.depth = depth
+        self.encoders = nn.ModuleList()
+        self.downsample = nn.ModuleList()
+        cin = int(input_channels)
+        for level, w in enumerate(widths):
+            self.encoders.append(ConvPair(cin, w, kernel_size, activation))
+            cin = w
+            if level + 1 < depth:
+                self.downsample.append(nn.Conv2d(w, widths[level + 1], kernel_size=2, stride=2))
+                cin = widths[level + 1]
+        self.upsample = nn.ModuleList()
+        self.decoders = nn.ModuleList()
+        for w in reversed(widths[:-1]):
+            self.upsample.append(nn.ConvTranspose2d(cin, w, kernel_size=2, stride=2))
+            self.decoders.append(ConvPair(2 * w, w, kernel_size, activation))
+            cin = w
+        self.residual_head = nn.Conv2d(cin, int(output_channels), kernel_size=1)
+        nn.init.zeros_(self.residual_head.weight)
+        nn.init.zeros_(self.residual_head.bias)
+
+    def forward(self, x: torch.Tensor) -> torch.Tensor:
+        skips = []
+        for level, enc in enumerate(self.encoders):
+            x = enc(x)
+            skips.append(x)
+            if level + 1 < self.depth:
+                x = self.downsample[level](pad_same_stride2(x))
+        for up, dec, skip in zip(self.upsample, self.decoders, reversed(skips[:-1])):
+            x = up(x)
+            if x.shape[-2:] != skip.shape[-2:]:
+                x = F.interpolate(x, size=skip.shape[-2:], mode="bilinear", align_corners=False)
+            x = dec(torch.cat((x, skip), dim=1))
+        return self.residual_head(x)
+
+
+def count_parameters(model: nn.Module) -> int:
+    return sum(p.numel() for p in model.parameters() if p.requires_grad)
+
+
+def corrector_4level(input_channels: int = 5, output_channels: int = 1) -> ResidualUNet:
+    """The 4-level (32, 64, 128, 256) corrector on (h, hu, hv, z, rain) -> depth."""
+    return ResidualUNet(input_channels=input_channels, depth=4, channels=(32, 64, 128, 256),
+                        output_channels=output_channels)

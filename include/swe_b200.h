@@ -180,6 +180,43 @@ int swe_rollout_backward(swe_domain_t d, const float *ckpt, int32_t ckpt_every, 
                          float *lam_hv, int64_t lam_pitch, float *grad_n2, double *grad_rain_scale,
                          float *seg, void *stream);
 
+/* Advance (h, hu, hv) IN PLACE from t_start to t_target with CFL-limited
+ * steps (dt = min(cfl_dt, t_target - t)), at most max_steps of them: the
+ * physics of one correction interval, advance_physics_to_time
+ * (hybrid/coupled_forecast.py:123-161), with a float64 clock.
+ * SWE_ERR_MAX_STEPS when the target was not reached within 1e-7 s. */
+int swe_advance_to(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, double t_start,
+                   double t_target, int32_t max_steps, swe_run_result *result, void *stream);
+
+#define SWE_FEATURES_REFERENCE6 0 /* (h,u,v) standardised, rain/scale, terrain, roughness */
+#define SWE_FEATURES_STATE5 1     /* (h, hu, hv, bed, rain mm/h), each standardised */
+
+/* Network input features of a state, channels-last [rows][cols][C] in
+ * float32 or bfloat16 (network_features, hybrid/coupled_forecast.py:53-79).
+ * mean/stddev: host float[3] (REFERENCE6: h, u, v) or float[5] (STATE5);
+ * rain_feature is the value of the rain channel (REFERENCE6: rate in mm/h
+ * over the rain scale; STATE5: rate in mm/h, standardised here);
+ * terrain/roughness: device rows*cols float32 (REFERENCE6 only, may be NULL). */
+int swe_network_features(swe_domain_t d, const float *h, const float *hu, const float *hv, int64_t pitch,
+                         int32_t layout, const float *mean, const float *stddev, float rain_feature,
+                         const float *terrain, const float *roughness, void *out, int32_t out_bf16,
+                         void *stream);
+
+/* Volume-preserving residual correction (apply_residual_correction,
+ * hybrid/coupled_forecast.py:82-120), with the clip of :199-200 fused in:
+ * res = clip(residual, -clip_limits, clip_limits) per channel (host
+ * float[res_channels], or NULL for none); h' = max(h + r*res_h, 0) on active
+ * cells, scaled back to the predicted water volume (sums in float64);
+ * velocities + r*res_(u,v) when res_channels == 3; momenta rebuilt on wet
+ * cells.  residual element (row, col, ch) is residual[row*sr + col*sc + ch*sch]
+ * in float32 or bfloat16 (residual_bf16), on the device.  Outputs may alias
+ * the inputs. */
+int swe_apply_correction(swe_domain_t d, const float *h, const float *hu, const float *hv, int64_t pitch,
+                         const void *residual, int32_t residual_bf16, int64_t res_stride_row,
+                         int64_t res_stride_col, int64_t res_stride_channel, int32_t res_channels,
+                         const float *clip_limits, double relaxation, float *h_out, float *hu_out,
+                         float *hv_out, int64_t out_pitch, void *stream);
+
 /* ---- Batched ensemble (no single counterpart in the reference: it batches many
  * reference runs -- NumpyShallowWaterSolver.run per member, numpy_solver/
  * shallow_water_2d.py:382-424 -- into one launch per step). ---- */
@@ -202,6 +239,17 @@ int swe_ensemble_advance(swe_ensemble_t e, float *const *h, float *const *hu, fl
                          const int64_t *pitch, int32_t n_steps, const double *start_s,
                          swe_run_result *results, void *stream);
 
+/* Advance every member IN PLACE from start_s[m] to target_s with CFL-limited
+ * steps, at most max_steps each: advance_physics_to_time
+ * (hybrid/coupled_forecast.py:123-161) for a batch of members, as 50-step
+ * graphs until all members are done.  SWE_ERR_MAX_STEPS when a member did not
+ * reach the target (its result says which). */
+int swe_ensemble_advance_to(swe_ensemble_t e, float *const *h, float *const *hu, float *const *hv,
+                            const int64_t *pitch, const double *start_s, double target_s, int32_t max_steps,
+                            swe_run_result *results, void *stream);
+/* Borrowed handle of member m (owned by the ensemble: do not destroy it), for
+ * the per-domain calls (features, correction, step, cfl). */
+int swe_ensemble_member(swe_ensemble_t e, int32_t m, swe_domain_t *out);
 int swe_ensemble_set_timing(swe_ensemble_t e, int32_t enable);
 int swe_ensemble_last_step_time(swe_ensemble_t e, double *ms, int64_t *steps);
 int64_t swe_ensemble_last_launch_count(swe_ensemble_t e);
