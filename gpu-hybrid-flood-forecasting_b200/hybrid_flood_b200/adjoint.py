@@ -57,6 +57,49 @@ def adjoint_step(solver, state: SWEState, lam: SWEState, dt: float, time_s: floa
     return SWEState(*out)
 
 
+class SWEStepFunction(torch.autograd.Function):
+    """One fixed-dt step ``finite_volume_step(state, params, dt, time_s)``
+    (``src/hybrid_flood/jax_solver/numerics.py:312-369``) as an autograd node.
+
+    forward(h, hu, hv, manning_n or None, solver, dt, time_s) -> (h', hu', hv').
+    Backward is the hand-written reverse step: gradients for the state and, when
+    ``manning_n`` is given, for the Manning field (dt is a stop-gradient).
+    """
+
+    @staticmethod
+    def forward(ctx, h, hu, hv, manning_n, solver, dt, time_s):
+        if manning_n is not None:
+            set_manning(solver, manning_n.detach())
+        state = SWEState(*(t.detach().to(torch.float32).contiguous() for t in (h, hu, hv)))
+        out = solver.step(state, float(dt), float(time_s))
+        ctx.solver = solver
+        ctx.meta = (float(dt), float(time_s))
+        ctx.save_for_backward(state.h, state.hu, state.hv, manning_n)
+        return out.h, out.hu, out.hv
+
+    @staticmethod
+    def backward(ctx, gh, ghu, ghv):
+        solver = ctx.solver
+        h, hu, hv, manning_n = ctx.saved_tensors
+        dt, t = ctx.meta
+        if manning_n is not None:
+            set_manning(solver, manning_n.detach())
+        lam = SWEState(*(torch.zeros_like(h) if g is None else g.detach().to(torch.float32).contiguous()
+                         for g in (gh, ghu, ghv)))
+        gn2 = torch.zeros_like(h)
+        gr = torch.zeros(1, dtype=torch.float64, device=h.device)
+        out = adjoint_step(solver, SWEState(h, hu, hv), lam, dt, t, gn2, gr)
+        grad_n = None
+        if manning_n is not None and ctx.needs_input_grad[3]:
+            grad_n = gn2 * 2.0 * manning_n.detach().to(torch.float32)
+        return out.h, out.hu, out.hv, grad_n, None, None, None
+
+
+def swe_step(solver, state, dt: float, time_s: float, manning_n=None) -> SWEState:
+    """Differentiable :meth:`B200ShallowWaterSolver.step` (see :class:`SWEStepFunction`)."""
+    return SWEState(*SWEStepFunction.apply(state[0], state[1], state[2], manning_n, solver, dt, time_s))
+
+
 class GaugeRollout(torch.autograd.Function):
     """Gauge depths of a fixed-dt rollout, differentiable in (n, h0, rain scale).
 

@@ -370,3 +370,71 @@ def rainfall_rate(params: DeviceParams, time_s: float) -> float:
     out = ctypes.c_double()
     _lib.check(lib.swe_rainfall_rate(h, float(time_s), ctypes.byref(out)), "rainfall_rate")
     return float(out.value)
+
+
+def benchmark_compiled_steps(solver: "B200ShallowWaterSolver", state, *, iterations: int = 100, dt_s: float = 1.0,
+                             output_directory=None) -> dict:
+    """Fixed-dt step timing (``src/hybrid_flood/jax_solver/benchmarking.py:17-97``).
+
+    ``iterations`` steps of ``dt_s`` from t = 0 (step k at time k*dt), run once
+    untimed and then timed with CUDA events on the solver's stream; the report
+    has the reference's fields.  The B200 path has no CPU backend, so the
+    ``cpu`` record says it is unavailable.
+    """
+    import datetime
+    import json
+    import pathlib
+
+    if iterations < 1:
+        raise ValueError("Benchmark iterations must be positive.")
+    dev = solver.device
+    base = _as_state(state, dev, solver.shape)
+    work = SWEState(*(t.clone().contiguous() for t in base))
+    lib = solver._lib
+
+    def once():
+        for t, b in zip(work, base):
+            t.copy_(b)
+        with torch.cuda.device(dev):
+            rc = lib.swe_rollout_forward(solver._handle, _ptr(work.h), _ptr(work.hu), _ptr(work.hv),
+                                         _pitch(work.h), int(iterations), float(dt_s), 0.0, None, 0, 1, None,
+                                         None, 1, _stream(dev))
+        _lib.check(rc, "benchmark_compiled_steps")
+
+    once()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for t, b in zip(work, base):
+        t.copy_(b)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    with torch.cuda.device(dev):
+        rc = lib.swe_rollout_forward(solver._handle, _ptr(work.h), _ptr(work.hu), _ptr(work.hv), _pitch(work.h),
+                                     int(iterations), float(dt_s), 0.0, None, 0, 1, None, None, 1, _stream(dev))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    _lib.check(rc, "benchmark_compiled_steps")
+    elapsed = e0.elapsed_time(e1) / 1e3
+    records = [
+        {"platform": "cpu", "available": False, "reason": "The B200 solver has no CPU backend."},
+        {"platform": "gpu", "available": True, "device": torch.cuda.get_device_name(dev),
+         "iterations": int(iterations), "total_seconds": elapsed, "seconds_per_step": elapsed / iterations,
+         "steps_per_second": iterations / elapsed, "grid_shape": list(solver.shape), "dtype": "float32",
+         "includes_jit_compilation": False, "arithmetic": solver.params.arithmetic},
+    ]
+    report = {
+        "generated_at": datetime.datetime.now(datetime.timezone.utc).isoformat(),
+        "library_version": lib.swe_version().decode(),
+        "default_backend": "gpu",
+        "devices": [torch.cuda.get_device_name(dev)],
+        "gpu_benchmark_available": True,
+        "benchmarks": records,
+    }
+    if output_directory is not None:
+        directory = pathlib.Path(output_directory)
+        directory.mkdir(parents=True, exist_ok=True)
+        stamp = datetime.datetime.now(datetime.timezone.utc).strftime("%Y%m%dT%H%M%S%fZ")
+        path = directory / f"benchmark_{stamp}.json"
+        path.write_text(json.dumps(report, indent=2, sort_keys=True), encoding="utf-8")
+        report["output_path"] = str(path)
+    return report

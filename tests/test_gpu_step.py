@@ -13,6 +13,8 @@ Tolerances (stated per test):
 
 from __future__ import annotations
 
+import pathlib
+
 import numpy as np
 import pytest
 import torch
@@ -278,3 +280,19 @@ def test_urban_2048_parity_and_invariants(cuda_device):
     assert t_end == pytest.approx(t, rel=1e-6)
     assert rel_l2(got.h.cpu().numpy(), st_o.h) < 1e-6
     assert ledger_error(led) < 1e-6
+
+
+def test_benchmark_compiled_steps_report(cuda_device, tmp_path):
+    """Fixed-dt timing helper with the fields of jax_solver/benchmarking.py:17-97."""
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver, benchmark_compiled_steps
+
+    z = golden("lake_gauss_20")
+    s = _solver(z, "fast")
+    with pytest.raises(ValueError):
+        benchmark_compiled_steps(s, list(z["state0"]), iterations=0)
+    rep = benchmark_compiled_steps(s, list(z["state0"]), iterations=20, dt_s=0.05, output_directory=tmp_path)
+    gpu = [r for r in rep["benchmarks"] if r["platform"] == "gpu"][0]
+    assert gpu["available"] and gpu["iterations"] == 20 and gpu["seconds_per_step"] > 0
+    assert gpu["grid_shape"] == list(z["state0"][0].shape)
+    assert rep["gpu_benchmark_available"] and pathlib.Path(rep["output_path"]).exists()
+    assert isinstance(s, B200ShallowWaterSolver)
