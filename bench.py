@@ -73,6 +73,9 @@ def _args():
     ap.add_argument("--hybrid-members", type=int, default=16)
     ap.add_argument("--hybrid-size", type=int, default=1024)
     ap.add_argument("--hybrid-intervals", type=int, default=10)
+    ap.add_argument("--no-training", action="store_true")
+    ap.add_argument("--training-members", type=int, default=16)
+    ap.add_argument("--training-size", type=int, default=1024)
     return ap.parse_args()
 
 
@@ -353,6 +356,55 @@ def _hybrid(args, dev):
             "cell_updates_per_s": phys_updates / (total_ms / 1e3), "finite": finite}
 
 
+def _training(args, dev):
+    """One optimiser step of the corrector trained THROUGH the solver: 16 urban
+    1024x1024 members, 10 correction intervals of 60 s, targets from 2x refined
+    (2048x2048, dx = 0.5 m) runs block-averaged back; bf16 4-level corrector."""
+    import torch
+
+    from hybrid_flood_b200.ensemble import B200Ensemble
+    from hybrid_flood_b200.hybrid import HybridInputs
+    from hybrid_flood_b200.training import refined_targets, train_step
+    from hybrid_flood_b200.unet import corrector_4level
+    from hybrid_flood_b200.workloads import as_member, street_depth, urban
+
+    torch.backends.cudnn.benchmark = True
+    M, S, K = args.training_members, args.training_size, args.hybrid_intervals
+    times = 60.0 * np.arange(K + 1)
+    ws = [urban(S, S, seed=3000 + m) for m in range(M)]
+    members = [as_member(w) for w in ws]
+    depths = [street_depth(w) for w in ws]
+    stream = torch.cuda.current_stream(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize(dev)
+    ev[0].record(stream)
+    targets = [refined_targets(mem, d0, times, device=dev) for mem, d0 in zip(members, depths)]
+    ev[1].record(stream)
+    ens = B200Ensemble(members, arithmetic=args.arith, device=dev)
+    states = [(d, np.zeros_like(d), np.zeros_like(d)) for d in depths]
+    z = np.stack([w.bed for w in ws])
+    h0 = np.stack(depths)
+    hi = HybridInputs(None, None, np.array([h0.mean(), 0.0, 0.0, z.mean(), 5.0], np.float32),
+                      np.array([max(h0.std(), 1e-3), 0.05, 0.05, max(z.std(), 1e-3), 5.0], np.float32),
+                      25.0, np.array([0.01], np.float32))
+    torch.manual_seed(0)
+    net = corrector_4level().to(device=dev, dtype=torch.bfloat16, memory_format=torch.channels_last)
+    opt = torch.optim.Adam(net.parameters(), lr=1e-4)
+    kw = dict(max_substeps_per_interval=5000, correction_relaxation=0.5, feature_layout="state5")
+    loss0, _ = train_step(ens, states, net, opt, hi, times, targets, **kw)  # warm-up: graphs, cuDNN plans
+    torch.cuda.synchronize(dev)
+    ev[2].record(stream)
+    loss1, steps = train_step(ens, states, net, opt, hi, times, targets, **kw)
+    ev[3].record(stream)
+    torch.cuda.synchronize(dev)
+    step_ms = ev[2].elapsed_time(ev[3])
+    return {"workload": f"{M} urban {S}x{S} members dx=1m, {K} intervals of 60 s, targets from 2x refined runs, "
+                        "bf16 4-level corrector, relaxation 0.5, Adam",
+            "members": M, "intervals": K, "train_step_ms": step_ms, "target_runs_ms": ev[0].elapsed_time(ev[1]),
+            "physics_steps_mean": float(steps.float().mean()), "loss_first": loss0, "loss_second": loss1,
+            "peak_mem_gb": torch.cuda.max_memory_allocated(dev) / 1e9}
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
@@ -463,6 +515,9 @@ def run_b200(args, rank: int, world: int):
     hyb = None
     if not args.no_hybrid and rank == 0:
         hyb = _hybrid(args, dev)
+    trn = None
+    if not args.no_training and rank == 0:
+        trn = _training(args, dev)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -496,6 +551,8 @@ def run_b200(args, rank: int, world: int):
         line["adjoint"] = adj
     if hyb:
         line["hybrid"] = hyb
+    if trn:
+        line["training"] = trn
     if not args.no_cpu_baseline:
         from oracle import cport
 

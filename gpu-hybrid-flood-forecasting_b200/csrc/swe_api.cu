@@ -262,7 +262,7 @@ int copy_plane(float* dst, int64_t dpitch, const float* src, int64_t spitch, int
 // ensemble.
 int begin_run(swe_domain* d, StateView init, const float* times_host, int n_times, double t_start,
               int n_out, int max_steps, float* out_h, float* out_hu, float* out_hv, cudaStream_t st,
-              const double* times64_host = nullptr) {
+              const double* times64_host = nullptr, double* dt_log = nullptr) {
     const int rows = d->dd.rows, cols = d->dd.cols;
     int rc = ensure_ping(d);
     if (rc) return rc;
@@ -303,6 +303,7 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
     c0.times = d->times_dev;
     c0.times64 = times64_host ? d->times64_dev : nullptr;
     c0.done_counter = d->done_counter;
+    c0.dt_log = dt_log;
     c0.out_h = out_h;
     c0.out_hu = out_hu;
     c0.out_hv = out_hv;
@@ -321,14 +322,14 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
 int run_driver(swe_domain* d, StateView init, const float* times_host, int n_times,
                double t_start, int n_out, int max_steps, float* out_h, float* out_hu,
                float* out_hv, swe_run_result* res, cudaStream_t st, int* final_buf,
-               const double* times64_host = nullptr) {
+               const double* times64_host = nullptr, double* dt_log = nullptr) {
     int rc = ensure_ping(d);
     if (rc) return rc;
     const Plan pl = make_plan(d, d->run_vec, true);
     rc = ensure_parts(d, std::max(pl.blocks, reduce_blocks(d)));
     if (rc) return rc;
     rc = begin_run(d, init, times_host, n_times, t_start, n_out, max_steps, out_h, out_hu, out_hv, st,
-                   times64_host);
+                   times64_host, dt_log);
     if (rc) return rc;
     int64_t launched = 0;
     d->launches = 1;
@@ -710,6 +711,14 @@ int noalloc_scratch(NoAllocScratch** out) {
 
 namespace {
 // Depth at flat cell indices (rows*cols numbering) of a pitched plane.
+// Clock at the start of step k of a fixed-dt (dts == null) or logged-dt rollout:
+// t_{k+1} = t_k + dt_k in float64, the accumulation the run-mode clock uses.
+double step_time(int k, double dt, double t0, const double* dts) {
+    double t = t0;
+    for (int j = 0; j < k; ++j) t += dts ? dts[j] : dt;
+    return t;
+}
+
 __global__ void gauge_gather_kernel(const float* h, int64_t pitch, int cols, const int64_t* idx, int n,
                                     float* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1102,7 +1111,7 @@ int swe_advance(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, i
 int64_t swe_last_launch_count(swe_domain_t d) { return d ? d->launches : -1; }
 
 int swe_advance_to(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, double t_start,
-                   double t_target, int32_t max_steps, swe_run_result* result, void* stream) {
+                   double t_target, int32_t max_steps, double* dt_log, swe_run_result* result, void* stream) {
     if (!d || !result) return fail(SWE_ERR_INVALID, "null argument");
     int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
     if (rc) return rc;
@@ -1112,7 +1121,7 @@ int swe_advance_to(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch
     const double times64[2] = {t_start, t_target};
     int fb = 0;
     rc = run_driver(d, StateView{h, hu, hv, pitch}, times, 2, t_start, 2, max_steps, nullptr, nullptr, nullptr,
-                    result, st, &fb, times64);
+                    result, st, &fb, times64, dt_log);
     if (rc) return rc;
     float* outs[3] = {h, hu, hv};
     for (int f = 0; f < 3; ++f) {
@@ -1215,7 +1224,7 @@ int swe_apply_correction(swe_domain_t d, const float* h, const float* hu, const 
 
 
 int swe_rollout_forward(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, int32_t n_steps,
-                        double dt, double t0, const int64_t* gauge_index, int32_t n_gauges,
+                        double dt, double t0, const double* dts, const int64_t* gauge_index, int32_t n_gauges,
                         int32_t obs_every, float* obs, float* ckpt, int32_t ckpt_every, void* stream) {
     if (!d) return fail(SWE_ERR_INVALID, "null domain");
     int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
@@ -1232,9 +1241,9 @@ int swe_rollout_forward(swe_domain_t d, float* h, float* hu, float* hv, int64_t 
         if (rc) return rc;
     }
     const int64_t plane = (int64_t)rows * cols;
-    double t = t0;
     for (int k = 0; k < n_steps; ++k) {
         const int src = k & 1;
+        const double t = step_time(k, dt, t0, dts), dtk = dts ? dts[k] : dt;
         if (ckpt && k % ckpt_every == 0) {
             float* dst = ckpt + (int64_t)(k / ckpt_every) * 3 * plane;
             for (int f = 0; f < 3; ++f) {
@@ -1243,9 +1252,8 @@ int swe_rollout_forward(swe_domain_t d, float* h, float* hu, float* hv, int64_t 
             }
         }
         rc = swe_step(d, d->ping[src][0], d->ping[src][1], d->ping[src][2], d->ppitch, d->ping[src ^ 1][0],
-                      d->ping[src ^ 1][1], d->ping[src ^ 1][2], d->ppitch, dt, t, stream);
+                      d->ping[src ^ 1][1], d->ping[src ^ 1][2], d->ppitch, dtk, t, stream);
         if (rc) return rc;
-        t += dt;
         if (n_gauges > 0 && (k + 1) % obs_every == 0) {
             gauge_gather_kernel<<<(n_gauges + 127) / 128, 128, 0, st>>>(
                 d->ping[src ^ 1][0], d->ppitch, cols, gauge_index, n_gauges,
@@ -1262,9 +1270,10 @@ int swe_rollout_forward(swe_domain_t d, float* h, float* hu, float* hv, int64_t 
 }
 
 int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, int32_t n_steps, double dt,
-                         double t0, const int64_t* gauge_index, int32_t n_gauges, int32_t obs_every,
-                         const float* grad_obs, float* lam_h, float* lam_hu, float* lam_hv, int64_t lam_pitch,
-                         float* grad_n2, double* grad_rain_scale, float* seg, void* stream) {
+                         double t0, const double* dts, const int64_t* gauge_index, int32_t n_gauges,
+                         int32_t obs_every, const float* grad_obs, float* lam_h, float* lam_hu, float* lam_hv,
+                         int64_t lam_pitch, int32_t lam_in, float* grad_n2, double* grad_rain_scale, float* seg,
+                         void* stream) {
     if (!d || !ckpt || !seg || ckpt_every < 1 || n_steps < 0) return fail(SWE_ERR_INVALID, "bad rollout arguments");
     if (n_gauges > 0 && (!gauge_index || !grad_obs || obs_every < 1)) return fail(SWE_ERR_INVALID, "bad gauge arguments");
     int rc = check_state_ptrs(lam_h, lam_hu, lam_hv, lam_pitch, d->dd.cols);
@@ -1273,8 +1282,9 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
     const int rows = d->dd.rows, cols = d->dd.cols;
     const int64_t plane = (int64_t)rows * cols;
     float* lam[3] = {lam_h, lam_hu, lam_hv};
-    for (int f = 0; f < 3; ++f)
-        SWE_CK(cudaMemset2DAsync(lam[f], sizeof(float) * lam_pitch, 0, sizeof(float) * cols, rows, st));
+    if (!lam_in)
+        for (int f = 0; f < 3; ++f)
+            SWE_CK(cudaMemset2DAsync(lam[f], sizeof(float) * lam_pitch, 0, sizeof(float) * cols, rows, st));
     const int nseg = n_steps > 0 ? (n_steps + ckpt_every - 1) / ckpt_every : 0;
     for (int sgi = nseg - 1; sgi >= 0; --sgi) {
         const int k0 = sgi * ckpt_every;
@@ -1285,8 +1295,8 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
         for (int k = k0; k < k1 - 1; ++k) {
             const float* a = seg + (int64_t)(k - k0) * 3 * plane;
             float* b = seg + (int64_t)(k + 1 - k0) * 3 * plane;
-            rc = swe_step(d, a, a + plane, a + 2 * plane, cols, b, b + plane, b + 2 * plane, cols, dt,
-                          t0 + k * dt, stream);
+            rc = swe_step(d, a, a + plane, a + 2 * plane, cols, b, b + plane, b + 2 * plane, cols,
+                          dts ? dts[k] : dt, step_time(k, dt, t0, dts), stream);
             if (rc) return rc;
         }
         for (int k = k1 - 1; k >= k0; --k) {
@@ -1297,8 +1307,8 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
             }
             const float* a = seg + (int64_t)(k - k0) * 3 * plane;
             rc = swe_adjoint_step(d, a, a + plane, a + 2 * plane, cols, lam_h, lam_hu, lam_hv, lam_pitch,
-                                  lam_h, lam_hu, lam_hv, lam_pitch, grad_n2, grad_rain_scale, dt,
-                                  t0 + k * dt, stream);
+                                  lam_h, lam_hu, lam_hv, lam_pitch, grad_n2, grad_rain_scale,
+                                  dts ? dts[k] : dt, step_time(k, dt, t0, dts), stream);
             if (rc) return rc;
         }
     }
@@ -1400,7 +1410,7 @@ int swe_ensemble_advance(swe_ensemble_t e, float* const* h, float* const* hu, fl
 
 int swe_ensemble_advance_to(swe_ensemble_t e, float* const* h, float* const* hu, float* const* hv,
                             const int64_t* pitch, const double* start_s, double target_s, int32_t max_steps,
-                            swe_run_result* results, void* stream) {
+                            double* const* dt_logs, swe_run_result* results, void* stream) {
     if (!e || !h || !hu || !hv || !pitch || !results || !start_s) return fail(SWE_ERR_INVALID, "null argument");
     if (max_steps < 0) return fail(SWE_ERR_INVALID, "max_steps must be >= 0");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1421,7 +1431,7 @@ int swe_ensemble_advance_to(swe_ensemble_t e, float* const* h, float* const* hu,
         const double times64[2] = {start_s[m], target_s};
         d->done_counter = e->done_counter;
         rc = begin_run(d, StateView{h[m], hu[m], hv[m], pitch[m]}, times, 2, start_s[m], 2, max_steps, nullptr,
-                       nullptr, nullptr, st, times64);
+                       nullptr, nullptr, st, times64, dt_logs ? dt_logs[m] : nullptr);
         d->done_counter = nullptr;
         if (rc) return rc;
     }

@@ -93,6 +93,7 @@ struct Control {
     const float* times;           // device copy of the float32 output times
     const double* times64;        // float64 targets instead of `times` (advance_to), or null
     unsigned* done_counter;       // incremented once when this run finishes (ensembles), or null
+    double* dt_log;               // dt of every planned step (index = step number), or null
     float* out_h;                 // n_out x rows x cols snapshots (may be null)
     float* out_hu;
     float* out_hv;
@@ -493,6 +494,7 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
         c.snap = -1;
         c.reach = -1;
     }
+    if (!c.done && c.dt_log) c.dt_log[c.steps] = c.dt;  // steps < max_steps while not done
     if (c.done && c.done_counter) atomicAdd(c.done_counter, 1u);
     *ctl = c;
     __threadfence();

@@ -134,12 +134,12 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_domain_set_manning": (ctypes.c_int, [_vp, _vp, _i32, _vp]),
         "swe_adjoint_step": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp,
                                             _i64, _vp, _vp, _f64, _f64, _vp]),
-        "swe_rollout_forward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _f64, _f64, _vp, _i32, _i32,
+        "swe_rollout_forward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _f64, _f64, _vp, _vp, _i32, _i32,
                                                _vp, _vp, _i32, _vp]),
-        "swe_rollout_backward": (ctypes.c_int, [_vp, _vp, _i32, _i32, _f64, _f64, _vp, _i32, _i32, _vp, _vp,
-                                                _vp, _vp, _i64, _vp, _vp, _vp, _vp]),
-        "swe_advance_to": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _f64, _f64, _i32, ctypes.POINTER(RunResult),
-                                          _vp]),
+        "swe_rollout_backward": (ctypes.c_int, [_vp, _vp, _i32, _i32, _f64, _f64, _vp, _vp, _i32, _i32, _vp, _vp,
+                                                _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp]),
+        "swe_advance_to": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _f64, _f64, _i32, _vp,
+                                          ctypes.POINTER(RunResult), _vp]),
         "swe_network_features": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _vp, _vp, ctypes.c_float, _vp,
                                                 _vp, _vp, _i32, _vp]),
         "swe_apply_correction": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _vp, _i32, _i64, _i64, _i64, _i32,
@@ -150,7 +150,7 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_ensemble_set_rows_per_warp": (ctypes.c_int, [_vp, _i32]),
         "swe_ensemble_advance": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp,
                                                 ctypes.POINTER(RunResult), _vp]),
-        "swe_ensemble_advance_to": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f64, _i32,
+        "swe_ensemble_advance_to": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f64, _i32, _vp,
                                                    ctypes.POINTER(RunResult), _vp]),
         "swe_ensemble_member": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_vp)]),
         "swe_ensemble_set_timing": (ctypes.c_int, [_vp, _i32]),

@@ -126,7 +126,7 @@ class GaugeRollout(torch.autograd.Function):
         with torch.cuda.device(dev):
             rc = solver._lib.swe_rollout_forward(
                 solver._handle, _ptr(state[0]), _ptr(state[1]), _ptr(state[2]), W, int(n_steps), float(dt),
-                float(start_time_s), _ptr(gauge_index), int(gauge_index.numel()), int(obs_every), _ptr(obs),
+                float(start_time_s), None, _ptr(gauge_index), int(gauge_index.numel()), int(obs_every), _ptr(obs),
                 _ptr(ckpt), int(checkpoint_every), _stream(dev))
         _lib.check(rc, "swe_rollout_forward")
         ctx.solver = solver
@@ -148,8 +148,8 @@ class GaugeRollout(torch.autograd.Function):
         g = grad_obs.detach().to(torch.float32).contiguous()
         with torch.cuda.device(dev):
             rc = solver._lib.swe_rollout_backward(
-                solver._handle, _ptr(ckpt), ckpt_every, n_steps, dt, t0, _ptr(gauge_index),
-                int(gauge_index.numel()), obs_every, _ptr(g), _ptr(lam[0]), _ptr(lam[1]), _ptr(lam[2]), W,
+                solver._handle, _ptr(ckpt), ckpt_every, n_steps, dt, t0, None, _ptr(gauge_index),
+                int(gauge_index.numel()), obs_every, _ptr(g), _ptr(lam[0]), _ptr(lam[1]), _ptr(lam[2]), W, 0,
                 _ptr(grad_n2), _ptr(grad_rain), _ptr(seg), _stream(dev))
         _lib.check(rc, "swe_rollout_backward")
         grad_n = grad_n2 * 2.0 * manning_n.detach().to(torch.float32)

@@ -89,6 +89,7 @@ class B200Ensemble:
         self.arithmetic = arithmetic
         self.rows_per_warp = 16
         self.dry_tolerances = [float(m.get("dry_tolerance_m", 1.0e-4)) for m in members]
+        self.beds = [np.asarray(m["bed"], dtype=np.float32) for m in members]
 
     def __del__(self):
         h = getattr(self, "_handle", None)
@@ -144,13 +145,14 @@ class B200Ensemble:
         return [(float(r.final_time_s), int(r.steps_used), dict(zip(LEDGER_KEYS, list(r.ledger)))) for r in res]
 
     def advance_to_(self, states: list[SWEState], start_times, target_time_s: float,
-                    max_steps: int) -> list[tuple]:
+                    max_steps: int, dt_logs: list | None = None) -> list[tuple]:
         """Advance every member IN PLACE from its start time to ``target_time_s``.
 
         At most ``max_steps`` CFL-limited steps per member; 50-step graphs are
         replayed until every member is done.  Returns one
         ``(final_time_s, steps_used, ledger)`` per member; a member stopped
-        short by the cap reports where it stopped.
+        short by the cap reports where it stopped.  ``dt_logs``: one device
+        float64 tensor of at least ``max_steps`` per member, receiving its dts.
         """
         n = len(self.shapes)
         if len(states) != n:
@@ -158,6 +160,12 @@ class B200Ensemble:
         self._check_states(states)
         starts = [float(start_times)] * n if np.isscalar(start_times) else [float(t) for t in start_times]
         arr = lambda typ, vals: (typ * n)(*vals)  # noqa: E731
+        logs = None
+        if dt_logs is not None:
+            if len(dt_logs) != n or not all(t.device == self.device and t.dtype == torch.float64
+                                            and t.is_contiguous() and t.numel() >= max_steps for t in dt_logs):
+                raise ValueError("dt_logs: one contiguous device float64 tensor of >= max_steps per member")
+            logs = arr(ctypes.c_void_p, [t.data_ptr() for t in dt_logs])
         res = (_lib.RunResult * n)()
         with torch.cuda.device(self.device):
             rc = self._lib.swe_ensemble_advance_to(
@@ -165,7 +173,7 @@ class B200Ensemble:
                 arr(ctypes.c_void_p, [s.hu.data_ptr() for s in states]),
                 arr(ctypes.c_void_p, [s.hv.data_ptr() for s in states]),
                 arr(ctypes.c_int64, [int(s.h.stride(0)) for s in states]), arr(ctypes.c_double, starts),
-                float(target_time_s), int(max_steps), res, _stream(self.device))
+                float(target_time_s), int(max_steps), logs, res, _stream(self.device))
         if rc != _lib.SWE_ERR_MAX_STEPS:
             _lib.check(rc, "swe_ensemble_advance_to")
         return [(float(r.final_time_s), int(r.steps_used), dict(zip(LEDGER_KEYS, list(r.ledger)))) for r in res]

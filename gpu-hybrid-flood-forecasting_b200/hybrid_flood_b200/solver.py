@@ -288,7 +288,7 @@ class B200ShallowWaterSolver:
         return float(res.final_time_s), int(res.steps_used), dict(zip(LEDGER_KEYS, list(res.ledger)))
 
     def advance_to_(self, state: SWEState, start_time_s: float, target_time_s: float,
-                    max_steps: int) -> tuple[float, int, dict]:
+                    max_steps: int, dt_log: torch.Tensor | None = None) -> tuple[float, int, dict]:
         """Advance ``state`` IN PLACE from ``start_time_s`` to ``target_time_s``.
 
         CFL-limited steps with ``dt = min(cfl_dt, target - t)``, at most
@@ -296,8 +296,12 @@ class B200ShallowWaterSolver:
         ``src/hybrid_flood/hybrid/coupled_forecast.py:123-161``).  Returns
         ``(final_time_s, steps_used, ledger)``; when the step cap stops the run
         short, ``final_time_s`` is where it stopped and the state is the one
-        reached there.
+        reached there.  ``dt_log`` (device float64, at least ``max_steps``
+        long) receives the dt of every step taken.
         """
+        if dt_log is not None and not (dt_log.device == self.device and dt_log.dtype == torch.float64
+                                       and dt_log.is_contiguous() and dt_log.numel() >= max_steps):
+            raise ValueError("dt_log must be a contiguous device float64 tensor of at least max_steps")
         res = _lib.RunResult()
         for t in state:
             if not (isinstance(t, torch.Tensor) and t.device == self.device and t.dtype == torch.float32
@@ -306,7 +310,8 @@ class B200ShallowWaterSolver:
         with torch.cuda.device(self.device):
             rc = self._lib.swe_advance_to(self._handle, _ptr(state.h), _ptr(state.hu), _ptr(state.hv),
                                           _pitch(state.h), float(start_time_s), float(target_time_s),
-                                          int(max_steps), ctypes.byref(res), _stream(self.device))
+                                          int(max_steps), _ptr(dt_log) if dt_log is not None else None,
+                                          ctypes.byref(res), _stream(self.device))
         if rc != _lib.SWE_ERR_MAX_STEPS:
             _lib.check(rc, "advance_to")
         return float(res.final_time_s), int(res.steps_used), dict(zip(LEDGER_KEYS, list(res.ledger)))
@@ -397,7 +402,7 @@ def benchmark_compiled_steps(solver: "B200ShallowWaterSolver", state, *, iterati
             t.copy_(b)
         with torch.cuda.device(dev):
             rc = lib.swe_rollout_forward(solver._handle, _ptr(work.h), _ptr(work.hu), _ptr(work.hv),
-                                         _pitch(work.h), int(iterations), float(dt_s), 0.0, None, 0, 1, None,
+                                         _pitch(work.h), int(iterations), float(dt_s), 0.0, None, None, 0, 1, None,
                                          None, 1, _stream(dev))
         _lib.check(rc, "benchmark_compiled_steps")
 
@@ -410,7 +415,7 @@ def benchmark_compiled_steps(solver: "B200ShallowWaterSolver", state, *, iterati
     e0.record(stream)
     with torch.cuda.device(dev):
         rc = lib.swe_rollout_forward(solver._handle, _ptr(work.h), _ptr(work.hu), _ptr(work.hv), _pitch(work.h),
-                                     int(iterations), float(dt_s), 0.0, None, 0, 1, None, None, 1, _stream(dev))
+                                     int(iterations), float(dt_s), 0.0, None, None, 0, 1, None, None, 1, _stream(dev))
     e1.record(stream)
     torch.cuda.synchronize(dev)
     _lib.check(rc, "benchmark_compiled_steps")

@@ -158,35 +158,41 @@ int swe_adjoint_step(swe_domain_t d, const float *h, const float *hu, const floa
                      float *lam_h_out, float *lam_hu_out, float *lam_hv_out, int64_t out_pitch,
                      float *grad_n2, double *grad_rain_scale, double dt, double time_s, void *stream);
 
-/* Fixed-dt rollout with gauge observations: the forward of the differentiable
- * rollout (no counterpart in the reference).  (h, hu, hv) advance IN PLACE by
- * n_steps steps of dt from t0.  Every obs_every steps the depths at the
- * n_gauges flat cell indices (device int64, row-major numbering) go to obs
- * (device float32 [n_steps/obs_every][n_gauges]).  If ckpt is non-NULL the
- * states at steps 0, ckpt_every, 2*ckpt_every, ... below n_steps are stored
- * there as [k][3][rows][cols]. */
+/* Fixed-dt (or logged-dt) rollout with gauge observations: the forward of the
+ * differentiable rollout (no counterpart in the reference).  (h, hu, hv)
+ * advance IN PLACE by n_steps steps from t0: of dt each, or of dts[k] (host
+ * float64 [n_steps], e.g. the log of an adaptive advance_to) when dts is
+ * non-NULL; the clock is accumulated in float64 as in the run loop.  Every
+ * obs_every steps the depths at the n_gauges flat cell indices (device int64,
+ * row-major numbering) go to obs (device float32 [n_steps/obs_every][n_gauges]).
+ * If ckpt is non-NULL the states at steps 0, ckpt_every, 2*ckpt_every, ...
+ * below n_steps are stored there as [k][3][rows][cols]. */
 int swe_rollout_forward(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, int32_t n_steps,
-                        double dt, double t0, const int64_t *gauge_index, int32_t n_gauges,
+                        double dt, double t0, const double *dts, const int64_t *gauge_index, int32_t n_gauges,
                         int32_t obs_every, float *obs, float *ckpt, int32_t ckpt_every, void *stream);
 
-/* Reverse of swe_rollout_forward: from its checkpoints and dL/dobs (device,
- * the layout of obs), writes dL/dU_0 to (lam_h, lam_hu, lam_hv), and ADDS
- * dL/d(n^2) into grad_n2 and dL/d(rain scale) into *grad_rain_scale.  Each
- * segment of ckpt_every steps is recomputed from its checkpoint into seg
- * (device, ckpt_every*3*rows*cols floats) and reversed step by step. */
+/* Reverse of swe_rollout_forward (same dt / dts): from its checkpoints and
+ * dL/dobs (device, the layout of obs), writes dL/dU_0 to (lam_h, lam_hu,
+ * lam_hv), and ADDS dL/d(n^2) into grad_n2 and dL/d(rain scale) into
+ * *grad_rain_scale.  lam_in = 1: the lam planes hold dL/dU_{n_steps} on entry
+ * (a loss on the final state); 0: they start at zero.  Each segment of
+ * ckpt_every steps is recomputed from its checkpoint into seg (device,
+ * ckpt_every*3*rows*cols floats) and reversed step by step. */
 int swe_rollout_backward(swe_domain_t d, const float *ckpt, int32_t ckpt_every, int32_t n_steps,
-                         double dt, double t0, const int64_t *gauge_index, int32_t n_gauges,
-                         int32_t obs_every, const float *grad_obs, float *lam_h, float *lam_hu,
-                         float *lam_hv, int64_t lam_pitch, float *grad_n2, double *grad_rain_scale,
-                         float *seg, void *stream);
+                         double dt, double t0, const double *dts, const int64_t *gauge_index,
+                         int32_t n_gauges, int32_t obs_every, const float *grad_obs, float *lam_h,
+                         float *lam_hu, float *lam_hv, int64_t lam_pitch, int32_t lam_in, float *grad_n2,
+                         double *grad_rain_scale, float *seg, void *stream);
 
 /* Advance (h, hu, hv) IN PLACE from t_start to t_target with CFL-limited
  * steps (dt = min(cfl_dt, t_target - t)), at most max_steps of them: the
  * physics of one correction interval, advance_physics_to_time
  * (hybrid/coupled_forecast.py:123-161), with a float64 clock.
+ * dt_log (device float64 [max_steps], or NULL) receives every step's dt, for
+ * replaying the interval (swe_rollout_forward/backward with dts).
  * SWE_ERR_MAX_STEPS when the target was not reached within 1e-7 s. */
 int swe_advance_to(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, double t_start,
-                   double t_target, int32_t max_steps, swe_run_result *result, void *stream);
+                   double t_target, int32_t max_steps, double *dt_log, swe_run_result *result, void *stream);
 
 #define SWE_FEATURES_REFERENCE6 0 /* (h,u,v) standardised, rain/scale, terrain, roughness */
 #define SWE_FEATURES_STATE5 1     /* (h, hu, hv, bed, rain mm/h), each standardised */
@@ -242,11 +248,12 @@ int swe_ensemble_advance(swe_ensemble_t e, float *const *h, float *const *hu, fl
 /* Advance every member IN PLACE from start_s[m] to target_s with CFL-limited
  * steps, at most max_steps each: advance_physics_to_time
  * (hybrid/coupled_forecast.py:123-161) for a batch of members, as 50-step
- * graphs until all members are done.  SWE_ERR_MAX_STEPS when a member did not
- * reach the target (its result says which). */
+ * graphs until all members are done.  dt_logs: NULL, or per member a device
+ * float64 [max_steps] log of its dts (as swe_advance_to).  SWE_ERR_MAX_STEPS
+ * when a member did not reach the target (its result says which). */
 int swe_ensemble_advance_to(swe_ensemble_t e, float *const *h, float *const *hu, float *const *hv,
                             const int64_t *pitch, const double *start_s, double target_s, int32_t max_steps,
-                            swe_run_result *results, void *stream);
+                            double *const *dt_logs, swe_run_result *results, void *stream);
 /* Borrowed handle of member m (owned by the ensemble: do not destroy it), for
  * the per-domain calls (features, correction, step, cfl). */
 int swe_ensemble_member(swe_ensemble_t e, int32_t m, swe_domain_t *out);
