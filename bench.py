@@ -273,7 +273,10 @@ def _adjoint(args, dev):
     stream = torch.cuda.current_stream(dev)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     with torch.no_grad():
-        gauge_rollout(solver, n_t, h_t, s_t, **kw)  # warm-up
+        gauge_rollout(solver, n_t, h_t, s_t, **kw)  # warm-up of the forward
+    warm = gauge_rollout(solver, n_t, h_t, s_t, **kw)  # and of the backward (scratch, plans)
+    torch.mean((warm - obs) ** 2).backward()
+    n_t.grad = h_t.grad = s_t.grad = None
     torch.cuda.synchronize(dev)
     ev[0].record(stream)
     with torch.no_grad():

@@ -11,7 +11,8 @@
 // lane copies its own two cells of the five input fields with cp.async (no
 // register is held while the copy is in flight) and waits with
 // cp.async.wait_group, a hardware wait with no polling.  Lanes past the right
-// edge copy nothing; their cells are filled from the last column (ghost ring).
+// edge copy zero bytes; their cells are filled from the last column (ghost
+// ring).
 #pragma once
 
 #include "swe_pair.cuh"
@@ -27,32 +28,8 @@ __device__ __forceinline__ KScalar make_kscalar(const Consts& k) {
     return {k.g, k.half_g, k.dry, k.eps, 0.f, 1.f, 1.0e-30f};
 }
 
-// Raw fields of the lane's two cells of row r (ghost ring applied), no velocities.
-__device__ __forceinline__ void load_pair_raw(const DomainDev& d, const StateView& s, int r, int c0,
-                                              CellT<float2>& c) {
-    Cell t[2];
-    load_cells<2>(d, s, r, c0, t);
-    c.h = f2(t[0].h, t[1].h);
-    c.hu = f2(t[0].hu, t[1].hu);
-    c.hv = f2(t[0].hv, t[1].hv);
-    c.z = f2(t[0].z, t[1].z);
-    c.nm = f2(t[0].nm, t[1].nm);
-}
+constexpr int kRing = 4;  // rows in flight per warp (a power of two)
 
-constexpr int kRing = 4;  // rows in flight per warp
-
-__device__ __forceinline__ void cp_async_8(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
-                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-                 "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_4(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
-                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-                 "l"(src)
-                 : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -71,293 +48,344 @@ struct WarpSmem {
     float2 ring[kRing][5][kWarp];  // [slot][field][lane]
 };
 
+__device__ __forceinline__ void cp_async_8z(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+// Ledger accumulation (float partials of diagnostics, not step arithmetic): packed FMA in both policies.
+__device__ __forceinline__ float2 lfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
 // One warp marches rows [r0, r1) of the 64-column strip starting at x0w: every
 // face once, cells updated, row r written to `out` (and to snapshot `snap` of
 // `ctl` in run mode); CFL maximum and ledger terms accumulate into `acc`.
+//
+// The row body has no data-dependent branch: partial lanes and boundary fluxes
+// are handled by per-lane float masks, ghost rows by a sign factor, and the
+// ring copies by their source size (zero bytes past the chunk or the right
+// edge).  The ledger terms accumulate as float partials over at most one
+// 32-row batch and are folded into the float64 accumulators per batch.
 template <class M, bool RUN, bool MASKED>
 __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& in,
-                                           const StateOut& out, const StepScalars& s, int snap,
-                                           double dtd, const Control* ctl, int r0, int r1,
-                                           int x0w, WarpSmem& sm, StepAccum& acc) {
+                                            const StateOut& out, const StepScalars& s, int snap,
+                                            double dtd, const Control* ctl, int r0, int r1,
+                                            int x0w, WarpSmem& sm, StepAccum& acc) {
     constexpr int kBatch = kWarp;
-    constexpr int V = 2;
     using A = P<M>;
     const Consts& k = d.k;
     const KPair kp = make_kpair(k);
     const KScalar ks = make_kscalar(k);
     const int lane = threadIdx.x & 31;
-    const int c0 = x0w + lane * V;
+    const int c0 = x0w + lane * 2;
     const B2 valid{c0 < d.cols, c0 + 1 < d.cols};
-    const int right_edge = d.cols - 1 - c0;  // 0 or 1 when this lane holds the last column
+    const float2 vmask = f2(valid.x ? 1.f : 0.f, valid.y ? 1.f : 0.f);
+    // The component holding the last column: its right x-face is the east boundary.
+    const float2 emask = f2(c0 == d.cols - 1 ? 1.f : 0.f, c0 + 1 == d.cols - 1 ? 1.f : 0.f);
     const float2 dt2 = splat(s.dt), dtr2 = splat(s.dt_rain), dtg2 = splat(s.dt_g);
     const float2 dx2 = splat(k.dx), dy2 = splat(k.dy);
     const float rdx = 1.0f / k.dx, rdy = 1.0f / k.dy;
     const float2 ndtdx2 = splat(-s.dt * rdx), ndtdy2 = splat(-s.dt * rdy);
     const float2 rdx2 = splat(rdx), rdy2 = splat(rdy);
     const float2 nexpo2 = splat(-k.expo);
+    const int nq = r1 - r0 + 2;  // rows r0-1 .. r1 pass through the ring
+    const bool edge_strip = x0w + kWarp * 2 > d.cols;
+    const int csize = valid.y ? 8 : (valid.x ? 4 : 0);
+    const int ccol = csize ? c0 : 0;  // copy source column (any aligned in-grid column when nothing is read)
+
+    // Start the copies of ring row qi (row r0-1+qi, clamped to the grid): one group per row,
+    // zero bytes past the chunk or the right edge, so the issue path has no branch.
+    auto issue = [&](int qi) {
+        const int q = r0 - 1 + qi;
+        const int rr = min(max(q, 0), d.rows - 1);
+        const int sz = qi < nq ? csize : 0;
+        const int slot = qi & (kRing - 1);
+        const int64_t so = (int64_t)rr * in.pitch + ccol, zo = (int64_t)rr * d.spitch + ccol;
+        cp_async_8z(&sm.ring[slot][0][lane], in.h + so, sz);
+        cp_async_8z(&sm.ring[slot][1][lane], in.hu + so, sz);
+        cp_async_8z(&sm.ring[slot][2][lane], in.hv + so, sz);
+        cp_async_8z(&sm.ring[slot][3][lane], d.bed + zo, sz);
+        cp_async_8z(&sm.ring[slot][4][lane], d.nm + zo, sz);
+        cp_async_commit();
+    };
+    // Ring row qi into registers, ghost ring applied; its slot is refilled with row qi+kRing.
+    auto consume = [&](int qi, CellT<float2>& c) {
+        cp_async_wait<kRing - 1>();
+        const int slot = qi & (kRing - 1);
+        const int q = r0 - 1 + qi;
+        float2 fv[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) fv[f] = sm.ring[slot][f][lane];
+        if (edge_strip) {
+            __syncwarp();  // the last column may sit in another lane's slot
+            const int last = d.cols - 1 - x0w;
+            const float* lastp = reinterpret_cast<const float*>(&sm.ring[slot][0][0]);
+            float g[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) g[f] = lastp[f * 2 * kWarp + last];
+            if (d.bnd[1] == 0) g[1] = -g[1];
+            if (c0 >= d.cols) {
+#pragma unroll
+                for (int f = 0; f < 5; ++f) fv[f].x = g[f];
+            }
+            if (c0 + 1 >= d.cols) {
+#pragma unroll
+                for (int f = 0; f < 5; ++f) fv[f].y = g[f];
+            }
+            __syncwarp();  // every lane has read before any slot is refilled
+        }
+        const float gs = ((q < 0 && d.bnd[2] == 0) || (q >= d.rows && d.bnd[3] == 0)) ? -1.f : 1.f;
+        c.h = fv[0];
+        c.hu = fv[1];
+        c.hv = A::mul(fv[2], splat(gs));
+        c.z = fv[3];
+        c.nm = fv[4];
+        set_vel_t<M>(c, kp);
+        issue(qi + kRing);
+    };
+
+    struct {
+        float2 vol, rain, clip, mask, out_x, out_y;
+    } lg;
+    auto zero_ledger = [&]() { lg.vol = lg.rain = lg.clip = lg.mask = lg.out_x = lg.out_y = kp.zero; };
+    zero_ledger();
+    float maxinv = 0.f;
+    // Float ledger partials cover at most one 32-row batch (64 cells per term), then go to float64.
+    auto flush_ledger = [&]() {
+        if constexpr (RUN) {
+            acc.vol += (double)lg.vol.x + (double)lg.vol.y;
+            acc.rain += (double)lg.rain.x + (double)lg.rain.y;
+            acc.clip += (double)lg.clip.x + (double)lg.clip.y;
+            acc.mask += (double)lg.mask.x + (double)lg.mask.y;
+            acc.outflow += dtd * ((double)(lg.out_x.x + lg.out_x.y) * d.dy + (double)(lg.out_y.x + lg.out_y.y) * d.dx);
+            zero_ledger();
+        }
+    };
+
+#pragma unroll
+    for (int qi = 0; qi < kRing; ++qi) issue(qi);
+
+    CellT<float2> R0, R1;
+    float2 yT0, yT1, yT2;
+    consume(0, R1);  // row r0-1
+    consume(1, R0);  // row r0
     {
-        const int nq = r1 - r0 + 2;  // rows r0-1 .. r1 pass through the ring
-        const float* planes[5] = {in.h, in.hu, in.hv, d.bed, d.nm};
-        const int64_t pitches[5] = {in.pitch, in.pitch, in.pitch, d.spitch, d.spitch};
-        const bool edge_strip = x0w + kWarp * V > d.cols;
-        // Start the copies of ring row qi (row r0-1+qi, clamped to the grid); one group per row.
-        auto issue = [&](int qi) {
-            if (qi < nq) {
-                const int q = r0 - 1 + qi;
-                const int rr = q < 0 ? 0 : (q >= d.rows ? d.rows - 1 : q);
-                const int st = qi % kRing;
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    const float* src = planes[f] + (int64_t)rr * pitches[f] + c0;
-                    if (c0 + 1 < d.cols) cp_async_8(&sm.ring[st][f][lane], src);
-                    else if (c0 < d.cols) cp_async_4(&sm.ring[st][f][lane], src);
-                }
-            }
-            cp_async_commit();
-        };
-        // Ring row qi into registers with the ghost ring applied; refill its slot.
-        auto consume = [&](int qi, CellT<float2>& out) {
-            cp_async_wait<kRing - 1>();
-            const int st = qi % kRing;
-            const int q = r0 - 1 + qi;
-            float2 fv[5];
-#pragma unroll
-            for (int f = 0; f < 5; ++f) fv[f] = sm.ring[st][f][lane];
-            if (edge_strip) {
-                __syncwarp();  // the last column may sit in another lane's slot
-                const int last = d.cols - 1 - x0w;
-                const float* lastp = reinterpret_cast<const float*>(&sm.ring[st][0][0]);
-                float g[5];
-#pragma unroll
-                for (int f = 0; f < 5; ++f) g[f] = lastp[f * 2 * kWarp + last];
-                if (d.bnd[1] == 0) g[1] = -g[1];
-                if (c0 >= d.cols) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) fv[f].x = g[f];
-                }
-                if (c0 + 1 >= d.cols) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) fv[f].y = g[f];
-                }
-                __syncwarp();  // every lane has read before any slot is refilled
-            }
-            if ((q < 0 && d.bnd[2] == 0) || (q >= d.rows && d.bnd[3] == 0)) fv[2] = neg(fv[2]);
-            out.h = fv[0];
-            out.hu = fv[1];
-            out.hv = fv[2];
-            out.z = fv[3];
-            out.nm = fv[4];
-            set_vel_t<M>(out, kp);
-            issue(qi + kRing);
-        };
-#pragma unroll
-        for (int qi = 0; qi < kRing; ++qi) issue(qi);
-
-        CellT<float2> Ab, Bb;
-        float2 yT0, yT1, yT2;
-        consume(0, Ab);  // row r0-1
-        consume(1, Bb);  // row r0
-        {
-            const FaceT<float2> f = face_t<0, M, MASKED>(Ab, Bb, kp);
-            yT0 = f.f0;
-            yT1 = f.f1;
-            yT2 = A::add(f.f2, f.corr_hi);
-            if (RUN && r0 == 0) {
-                if (valid.x) acc.outflow -= dtd * (double)f.f0.x * d.dx;
-                if (valid.y) acc.outflow -= dtd * (double)f.f0.y * d.dx;
-            }
+        const FaceT<float2> f = face_t<0, M, MASKED>(R1, R0, kp);
+        yT0 = f.f0;
+        yT1 = f.f1;
+        yT2 = A::add(f.f2, f.corr_hi);
+        if constexpr (RUN) {
+            if (r0 == 0) lg.out_y = lfma(neg(f.f0), vmask, lg.out_y);
         }
-        consume(2, Ab);  // row r0+1
-
-        auto row = [&](const int r, CellT<float2>& cur, CellT<float2>& nxt) {
-            const int j = (r - r0) & (kBatch - 1);
-            if (j == 0) {
-                // Strip edges for rows r .. r+31, one row per lane.
-                __syncwarp();
-                const int rr = min(r + lane, d.rows - 1);
-                Cell L[1], E[1], R[1];
-                load_cells<1>(d, in, rr, x0w - 1, L);
-                load_cells<1>(d, in, rr, x0w, E);
-                load_cells<1>(d, in, rr, x0w + kWarp * V, R);
-                CellT<float> l{L[0].h, L[0].hu, L[0].hv, L[0].z, L[0].nm, 0.f, 0.f};
-                CellT<float> e{E[0].h, E[0].hu, E[0].hv, E[0].z, E[0].nm, 0.f, 0.f};
-                CellT<float> q{R[0].h, R[0].hu, R[0].hv, R[0].z, R[0].nm, 0.f, 0.f};
-                set_vel_t<M>(l, ks);
-                set_vel_t<M>(e, ks);
-                set_vel_t<M>(q, ks);
-                const FaceT<float> f = face_t<1, M, MASKED>(l, e, ks);
-                sm.left[0][lane] = f.f0;
-                sm.left[1][lane] = A::add(f.f1, f.corr_hi);
-                sm.left[2][lane] = f.f2;
-                if (RUN && x0w == 0 && r + lane < r1) acc.outflow -= dtd * (double)f.f0 * d.dy;
-                sm.right[0][lane] = q.h;
-                sm.right[1][lane] = q.hu;
-                sm.right[2][lane] = q.hv;
-                sm.right[3][lane] = q.z;
-                sm.right[4][lane] = q.nm;
-                sm.right[5][lane] = q.u;
-                sm.right[6][lane] = q.v;
-                __syncwarp();
-            }
-
-            // y-faces above both columns: lo side for row r, hi side carried to row r+1.
-            const FaceT<float2> fy = face_t<0, M, MASKED>(cur, nxt, kp);
-            const float2 yB0 = fy.f0, yB1 = fy.f1, yB2 = A::add(fy.f2, fy.corr_lo);
-            const float2 yN2 = A::add(fy.f2, fy.corr_hi);
-            if (RUN && r == d.rows - 1) {
-                if (valid.x) acc.outflow += dtd * (double)fy.f0.x * d.dx;
-                if (valid.y) acc.outflow += dtd * (double)fy.f0.y * d.dx;
-            }
-
-            // x-faces: (cell 0 | cell 1) and (cell 1 | first cell of the next lane).
-            float rh = __shfl_down_sync(0xffffffffu, cur.h.x, 1);
-            float rhu = __shfl_down_sync(0xffffffffu, cur.hu.x, 1);
-            float rhv = __shfl_down_sync(0xffffffffu, cur.hv.x, 1);
-            float rz = __shfl_down_sync(0xffffffffu, cur.z.x, 1);
-            float rnm = __shfl_down_sync(0xffffffffu, cur.nm.x, 1);
-            float ru = __shfl_down_sync(0xffffffffu, cur.u.x, 1);
-            float rv = __shfl_down_sync(0xffffffffu, cur.v.x, 1);
-            {
-                const float e0 = sm.right[0][j], e1 = sm.right[1][j], e2 = sm.right[2][j];
-                const float e3 = sm.right[3][j], e4 = sm.right[4][j], e5 = sm.right[5][j];
-                const float e6 = sm.right[6][j];
-                if (lane == 31) {
-                    rh = e0; rhu = e1; rhv = e2; rz = e3; rnm = e4; ru = e5; rv = e6;
-                }
-            }
-            CellT<float2> xhi;
-            xhi.h = f2(cur.h.y, rh);
-            xhi.hu = f2(cur.hu.y, rhu);
-            xhi.hv = f2(cur.hv.y, rhv);
-            xhi.z = f2(cur.z.y, rz);
-            xhi.nm = f2(cur.nm.y, rnm);
-            xhi.u = f2(cur.u.y, ru);
-            xhi.v = f2(cur.v.y, rv);
-            const FaceT<float2> fx = face_t<1, M, MASKED>(cur, xhi, kp);
-            const float2 xl0 = fx.f0, xl1 = A::add(fx.f1, fx.corr_lo), xl2 = fx.f2;
-            const float2 xh1 = A::add(fx.f1, fx.corr_hi);
-            float up0 = __shfl_up_sync(0xffffffffu, fx.f0.y, 1);
-            float up1 = __shfl_up_sync(0xffffffffu, xh1.y, 1);
-            float up2 = __shfl_up_sync(0xffffffffu, fx.f2.y, 1);
-            {
-                const float l0 = sm.left[0][j], l1 = sm.left[1][j], l2 = sm.left[2][j];
-                if (lane == 0) {
-                    up0 = l0; up1 = l1; up2 = l2;
-                }
-            }
-            const float2 xr0 = f2(up0, fx.f0.x), xr1 = f2(up1, xh1.x), xr2 = f2(up2, fx.f2.x);
-            if (RUN && (right_edge == 0 || right_edge == 1))
-                acc.outflow += dtd * (double)(right_edge == 0 ? fx.f0.x : fx.f0.y) * d.dy;
-
-            // Cell updates of both columns.
-            const auto act = MASKED ? act_of(cur.nm) : all_true<float2>();
-            const float2 n2 = MASKED ? vabs(cur.nm) : cur.nm;
-            float2 u0, u1, u2;
-            if constexpr (A::kExact) {
-                u0 = A::sub(cur.h, A::mul(dt2, A::add(A::div(A::sub(xl0, xr0), dx2), A::div(A::sub(yB0, yT0), dy2))));
-                u1 = A::sub(cur.hu, A::mul(dt2, A::add(A::div(A::sub(xl1, xr1), dx2), A::div(A::sub(yB1, yT1), dy2))));
-                u2 = A::sub(cur.hv, A::mul(dt2, A::add(A::div(A::sub(xl2, xr2), dx2), A::div(A::sub(yB2, yT2), dy2))));
-            } else {
-                u0 = A::fma(ndtdx2, A::sub(xl0, xr0), A::fma(ndtdy2, A::sub(yB0, yT0), cur.h));
-                u1 = A::fma(ndtdx2, A::sub(xl1, xr1), A::fma(ndtdy2, A::sub(yB1, yT1), cur.hu));
-                u2 = A::fma(ndtdx2, A::sub(xl2, xr2), A::fma(ndtdy2, A::sub(yB2, yT2), cur.hv));
-            }
-            float2 rain;
-            if (d.mult != nullptr) {
-                const int64_t mo = (int64_t)r * d.spitch;
-                const float m0 = __ldg(d.mult + mo + min(c0, d.cols - 1));
-                const float m1 = __ldg(d.mult + mo + min(c0 + 1, d.cols - 1));
-                rain = A::mul(dtr2, f2(m0, m1));
-            } else {
-                rain = sel(act, dtr2, kp.zero);
-            }
-            u0 = A::add(u0, rain);
-            const float2 h = vmax(u0, kp.zero);
-            float2 qx, qy;
-            if constexpr (A::kExact) {
-                const float2 norm = A::hypot(u1, u2);
-                const float2 fr = A::div(A::mul(A::mul(dtg2, n2), norm), A::pow73(vmax(h, kp.dry), k.expo));
-                const float2 den = A::add(kp.one, fr);
-                qx = A::div(u1, den);
-                qy = A::div(u2, den);
-            } else {
-                const float2 norm = A::sqrt(A::fma(u1, u1, A::mul(u2, u2)));
-                const float2 hm = A::ex2(A::mul(A::lg2(vmax(h, kp.dry)), nexpo2));  // max(h,dry)^(-7/3)
-                const float2 fr = A::mul(A::mul(A::mul(dtg2, n2), norm), hm);
-                const float2 rd = A::rcp(A::add(kp.one, fr));
-                qx = A::mul(u1, rd);
-                qy = A::mul(u2, rd);
-            }
-            const auto wet = act & gt(h, kp.dry);
-            const float2 ho = sel(act, h, kp.zero);
-            const float2 huo = sel(wet, qx, kp.zero);
-            const float2 hvo = sel(wet, qy, kp.zero);
-            if constexpr (RUN) {
-                CellT<float2> nc;
-                nc.h = ho;
-                nc.hu = huo;
-                nc.hv = hvo;
-                set_vel_t<M>(nc, kp);
-                const float2 w = A::sqrt(A::mul(kp.g, ho));
-                float2 inv;
-                if constexpr (A::kExact) {
-                    inv = A::add(A::div(A::add(vabs(nc.u), w), dx2), A::div(A::add(vabs(nc.v), w), dy2));
-                } else {
-                    inv = A::fma(A::add(vabs(nc.u), w), rdx2, A::mul(A::add(vabs(nc.v), w), rdy2));
-                }
-                const auto use = act & valid;
-                acc.maxinv = nan_max(acc.maxinv, use.x ? inv.x : 0.0f);
-                acc.maxinv = nan_max(acc.maxinv, use.y ? inv.y : 0.0f);
-                acc.vol += (double)(valid.x ? ho.x : 0.0f) + (double)(valid.y ? ho.y : 0.0f);
-                if (d.mult != nullptr) {
-                    acc.rain += (double)(valid.x ? rain.x : 0.0f) + (double)(valid.y ? rain.y : 0.0f);
-                } else {
-                    acc.rain_cells += (use.x ? 1u : 0u) + (use.y ? 1u : 0u);
-                }
-                if (valid.x && u0.x < 0.0f) acc.clip -= (double)u0.x;
-                if (valid.y && u0.y < 0.0f) acc.clip -= (double)u0.y;
-                if (MASKED) {
-                    if (valid.x && !act.x) acc.mask += (double)h.x;
-                    if (valid.y && !act.y) acc.mask += (double)h.y;
-                }
-            }
-            const int64_t so = (int64_t)r * out.pitch;
-            if (c0 + 2 <= d.cols) {
-                *reinterpret_cast<float2*>(out.h + so + c0) = ho;
-                *reinterpret_cast<float2*>(out.hu + so + c0) = huo;
-                *reinterpret_cast<float2*>(out.hv + so + c0) = hvo;
-            } else if (valid.x) {
-                out.h[so + c0] = ho.x;
-                out.hu[so + c0] = huo.x;
-                out.hv[so + c0] = hvo.x;
-            }
-            if (RUN && snap >= 0) {
-                const Control* c = ctl;
-                const int64_t base = (int64_t)snap * c->out_plane + (int64_t)r * d.cols + c0;
-                if (valid.x) {
-                    c->out_h[base] = ho.x;
-                    c->out_hu[base] = huo.x;
-                    c->out_hv[base] = hvo.x;
-                }
-                if (valid.y) {
-                    c->out_h[base + 1] = ho.y;
-                    c->out_hu[base + 1] = huo.y;
-                    c->out_hv[base + 1] = hvo.y;
-                }
-            }
-            yT0 = fy.f0;
-            yT1 = fy.f1;
-            yT2 = yN2;
-            // Row r+2 takes over the registers row r leaves free.
-            if (r + 1 < r1) consume(r + 3 - r0, cur);
-        };
-
-        for (int r = r0; r < r1; r += 2) {
-            row(r, Bb, Ab);
-            if (r + 1 < r1) row(r + 1, Ab, Bb);
-        }
-        cp_async_wait<0>();  // nothing may land after the warp is done
     }
+    consume(2, R1);  // row r0+1
+
+    // The x-faces of a row: (cell 0 | cell 1) and (cell 1 | first cell of the next lane).
+    // Returns the lo-side fluxes of both cells' left faces and the hi-side of their right faces.
+    struct XF {
+        float2 l0, l1, l2;  // flux entering through each cell's left face (hi side of that face)
+        float2 r0, r1, r2;  // flux leaving through each cell's right face (lo side)
+        float2 e0;          // mass flux through each cell's right face (east outflow)
+    };
+    auto xfaces = [&](const CellT<float2>& cur, int j) -> XF {
+        float rh = __shfl_down_sync(0xffffffffu, cur.h.x, 1);
+        float rhu = __shfl_down_sync(0xffffffffu, cur.hu.x, 1);
+        float rhv = __shfl_down_sync(0xffffffffu, cur.hv.x, 1);
+        float rz = __shfl_down_sync(0xffffffffu, cur.z.x, 1);
+        float rnm = __shfl_down_sync(0xffffffffu, cur.nm.x, 1);
+        float ru = __shfl_down_sync(0xffffffffu, cur.u.x, 1);
+        float rv = __shfl_down_sync(0xffffffffu, cur.v.x, 1);
+        if (lane == 31) {
+            rh = sm.right[0][j]; rhu = sm.right[1][j]; rhv = sm.right[2][j]; rz = sm.right[3][j];
+            rnm = sm.right[4][j]; ru = sm.right[5][j]; rv = sm.right[6][j];
+        }
+        CellT<float2> xhi;
+        xhi.h = f2(cur.h.y, rh);
+        xhi.hu = f2(cur.hu.y, rhu);
+        xhi.hv = f2(cur.hv.y, rhv);
+        xhi.z = f2(cur.z.y, rz);
+        xhi.nm = f2(cur.nm.y, rnm);
+        xhi.u = f2(cur.u.y, ru);
+        xhi.v = f2(cur.v.y, rv);
+        const FaceT<float2> fx = face_t<1, M, MASKED>(cur, xhi, kp);
+        const float2 xh1 = A::add(fx.f1, fx.corr_hi);
+        float up0 = __shfl_up_sync(0xffffffffu, fx.f0.y, 1);
+        float up1 = __shfl_up_sync(0xffffffffu, xh1.y, 1);
+        float up2 = __shfl_up_sync(0xffffffffu, fx.f2.y, 1);
+        if (lane == 0) {
+            up0 = sm.left[0][j]; up1 = sm.left[1][j]; up2 = sm.left[2][j];
+        }
+        XF x;
+        x.r0 = fx.f0;
+        x.r1 = A::add(fx.f1, fx.corr_lo);
+        x.r2 = fx.f2;
+        x.l0 = f2(up0, fx.f0.x);
+        x.l1 = f2(up1, xh1.x);
+        x.l2 = f2(up2, fx.f2.x);
+        x.e0 = fx.f0;
+        return x;
+    };
+
+    struct Row {
+        float2 h, hu, hv;
+    };
+    // Cell update of one row from its faces: bottom (b*), top (t*, lo side), x-faces.
+    auto update = [&](int r, const CellT<float2>& cur, float2 b0, float2 b1, float2 b2, float2 t0, float2 t1,
+                      float2 t2, const XF& x) -> Row {
+        const auto act = MASKED ? act_of(cur.nm) : all_true<float2>();
+        const float2 n2 = MASKED ? vabs(cur.nm) : cur.nm;
+        float2 u0, u1, u2;
+        if constexpr (A::kExact) {
+            u0 = A::sub(cur.h, A::mul(dt2, A::add(A::div(A::sub(x.r0, x.l0), dx2), A::div(A::sub(t0, b0), dy2))));
+            u1 = A::sub(cur.hu, A::mul(dt2, A::add(A::div(A::sub(x.r1, x.l1), dx2), A::div(A::sub(t1, b1), dy2))));
+            u2 = A::sub(cur.hv, A::mul(dt2, A::add(A::div(A::sub(x.r2, x.l2), dx2), A::div(A::sub(t2, b2), dy2))));
+        } else {
+            u0 = A::fma(ndtdx2, A::sub(x.r0, x.l0), A::fma(ndtdy2, A::sub(t0, b0), cur.h));
+            u1 = A::fma(ndtdx2, A::sub(x.r1, x.l1), A::fma(ndtdy2, A::sub(t1, b1), cur.hu));
+            u2 = A::fma(ndtdx2, A::sub(x.r2, x.l2), A::fma(ndtdy2, A::sub(t2, b2), cur.hv));
+        }
+        float2 rain = sel(act, dtr2, kp.zero);
+        if (d.mult != nullptr) {
+            const int64_t mo = (int64_t)r * d.spitch;
+            rain = A::mul(dtr2, f2(__ldg(d.mult + mo + min(c0, d.cols - 1)), __ldg(d.mult + mo + min(c0 + 1, d.cols - 1))));
+        }
+        u0 = A::add(u0, rain);
+        const float2 h = vmax(u0, kp.zero);
+        float2 qx, qy;
+        if constexpr (A::kExact) {
+            const float2 norm = A::hypot(u1, u2);
+            const float2 fr = A::div(A::mul(A::mul(dtg2, n2), norm), A::pow73(vmax(h, kp.dry), k.expo));
+            const float2 den = A::add(kp.one, fr);
+            qx = A::div(u1, den);
+            qy = A::div(u2, den);
+        } else {
+            const float2 norm = A::sqrt(A::fma(u1, u1, A::mul(u2, u2)));
+            const float2 hm = A::ex2(A::mul(A::lg2(vmax(h, kp.dry)), nexpo2));  // max(h,dry)^(-7/3)
+            const float2 fr = A::mul(A::mul(A::mul(dtg2, n2), norm), hm);
+            const float2 rd = A::rcp(A::add(kp.one, fr));
+            qx = A::mul(u1, rd);
+            qy = A::mul(u2, rd);
+        }
+        const auto wet = act & gt(h, kp.dry);
+        Row o;
+        o.h = sel(act, h, kp.zero);
+        o.hu = sel(wet, qx, kp.zero);
+        o.hv = sel(wet, qy, kp.zero);
+        if constexpr (RUN) {
+            CellT<float2> nc;
+            nc.h = o.h;
+            nc.hu = o.hu;
+            nc.hv = o.hv;
+            set_vel_t<M>(nc, kp);
+            const float2 w = A::sqrt(A::mul(kp.g, o.h));
+            float2 inv;
+            if constexpr (A::kExact) {
+                inv = A::add(A::div(A::add(vabs(nc.u), w), dx2), A::div(A::add(vabs(nc.v), w), dy2));
+            } else {
+                inv = A::fma(A::add(vabs(nc.u), w), rdx2, A::mul(A::add(vabs(nc.v), w), rdy2));
+            }
+            // Inactive cells have h = hu = hv = 0 and so inv = 0; lanes past the edge are masked.
+            inv = A::mul(inv, vmask);
+            maxinv = nan_max(maxinv, inv.x);
+            maxinv = nan_max(maxinv, inv.y);
+            lg.vol = lfma(o.h, vmask, lg.vol);
+            if (d.mult != nullptr) lg.rain = lfma(rain, vmask, lg.rain);
+            lg.clip = lfma(neg(vmin(u0, kp.zero)), vmask, lg.clip);
+            if constexpr (MASKED) {
+                lg.mask = lfma(sel(act, kp.zero, h), vmask, lg.mask);
+                if (d.mult == nullptr) acc.rain_cells += (act.x && valid.x ? 1u : 0u) + (act.y && valid.y ? 1u : 0u);
+            }
+            lg.out_x = lfma(x.e0, emask, lg.out_x);
+        }
+        return o;
+    };
+    auto store = [&](int r, const Row& o) {
+        const int64_t so = (int64_t)r * out.pitch + c0;
+        if (valid.y) {
+            *reinterpret_cast<float2*>(out.h + so) = o.h;
+            *reinterpret_cast<float2*>(out.hu + so) = o.hu;
+            *reinterpret_cast<float2*>(out.hv + so) = o.hv;
+        } else if (valid.x) {
+            out.h[so] = o.h.x;
+            out.hu[so] = o.hu.x;
+            out.hv[so] = o.hv.x;
+        }
+        if (RUN && snap >= 0) {
+            const Control* c = ctl;
+            const int64_t base = (int64_t)snap * c->out_plane + (int64_t)r * d.cols + c0;
+            if (valid.x) {
+                c->out_h[base] = o.h.x;
+                c->out_hu[base] = o.hu.x;
+                c->out_hv[base] = o.hv.x;
+            }
+            if (valid.y) {
+                c->out_h[base + 1] = o.h.y;
+                c->out_hu[base + 1] = o.hu.y;
+                c->out_hv[base + 1] = o.hv.y;
+            }
+        }
+    };
+    // Strip edges for rows rb .. rb+31, one row per lane (the left x-face and the right halo cell).
+    auto batch = [&](int rb) {
+        __syncwarp();
+        const int rr = min(rb + lane, d.rows - 1);
+        Cell L[1], E[1], Q[1];
+        load_cells<1>(d, in, rr, x0w - 1, L);
+        load_cells<1>(d, in, rr, x0w, E);
+        load_cells<1>(d, in, rr, x0w + kWarp * 2, Q);
+        CellT<float> l{L[0].h, L[0].hu, L[0].hv, L[0].z, L[0].nm, 0.f, 0.f};
+        CellT<float> e{E[0].h, E[0].hu, E[0].hv, E[0].z, E[0].nm, 0.f, 0.f};
+        CellT<float> q{Q[0].h, Q[0].hu, Q[0].hv, Q[0].z, Q[0].nm, 0.f, 0.f};
+        set_vel_t<M>(l, ks);
+        set_vel_t<M>(e, ks);
+        set_vel_t<M>(q, ks);
+        const FaceT<float> f = face_t<1, M, MASKED>(l, e, ks);
+        sm.left[0][lane] = f.f0;
+        sm.left[1][lane] = A::add(f.f1, f.corr_hi);
+        sm.left[2][lane] = f.f2;
+        if (RUN && x0w == 0 && rb + lane < r1) lg.out_x.x -= f.f0;
+        sm.right[0][lane] = q.h;
+        sm.right[1][lane] = q.hu;
+        sm.right[2][lane] = q.hv;
+        sm.right[3][lane] = q.z;
+        sm.right[4][lane] = q.nm;
+        sm.right[5][lane] = q.u;
+        sm.right[6][lane] = q.v;
+        __syncwarp();
+    };
+
+    // One row: `cur` is row r, `nxt` row r+1; afterwards `cur` receives row r+2.
+    auto row = [&](const int r, const int j, CellT<float2>& cur, const CellT<float2>& nxt) {
+        const FaceT<float2> fy = face_t<0, M, MASKED>(cur, nxt, kp);
+        const XF x = xfaces(cur, j);
+        const Row o = update(r, cur, yT0, yT1, yT2, fy.f0, fy.f1, A::add(fy.f2, fy.corr_lo), x);
+        if constexpr (RUN) {
+            const float top = r == d.rows - 1 ? 1.f : 0.f;
+            lg.out_y = lfma(fy.f0, __fmul2_rn(vmask, splat(top)), lg.out_y);
+        }
+        yT0 = fy.f0;
+        yT1 = fy.f1;
+        yT2 = A::add(fy.f2, fy.corr_hi);
+        store(r, o);
+        if (r + 1 < r1) consume(r + 3 - r0, cur);
+    };
+    for (int rb = r0; rb < r1; rb += kBatch) {
+        flush_ledger();
+        batch(rb);
+        const int re = min(rb + kBatch, r1);
+        for (int r = rb; r < re; r += 2) {
+            row(r, r - rb, R0, R1);
+            if (r + 1 < re) row(r + 1, r + 1 - rb, R1, R0);
+        }
+    }
+    flush_ledger();
+    if constexpr (RUN) {
+        acc.maxinv = nan_max(acc.maxinv, maxinv);
+        // Without a mask every in-grid cell of every row received dt*rate.
+        if (!MASKED && d.mult == nullptr) acc.rain_cells += (unsigned)((valid.x ? 1 : 0) + (valid.y ? 1 : 0)) * (unsigned)(r1 - r0);
+    }
+    cp_async_wait<0>();  // nothing may land after the warp is done
 }
 
 template <class M, int THREADS, bool RUN, bool MASKED>
@@ -385,7 +413,7 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
     acc.zero();
     if (r0 < d.rows)
         march_pair<M, RUN, MASKED>(d, p.in, p.out, s, snap, dtd, p.ctl, r0, r1, strip * kWarp * 2,
-                                   s_warp[wib], acc);
+                                  s_warp[wib], acc);
     if constexpr (RUN) {
         Accum a;
         a.maxinv = acc.maxinv;
@@ -419,8 +447,13 @@ struct MemberDev {
     int nstrips, rows_per_warp, ncta;
 };
 
+// The ensemble kernel keeps its member record in registers on top of the
+// march: at 4 CTAs/SM (128 registers) it spills, at 3 it does not and is faster.
+#ifndef SWE_ENS_MINBLOCKS
+#define SWE_ENS_MINBLOCKS 3
+#endif
 template <class M, int THREADS, bool MASKED>
-__global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS)
+__global__ void __launch_bounds__(THREADS, SWE_ENS_MINBLOCKS)
 ensemble_step_kernel(const MemberDev* __restrict__ members, const int2* __restrict__ items,
                      int n_items, int parity) {
     constexpr int NW = THREADS / kWarp;

@@ -67,7 +67,10 @@ def test_exact_ensemble_members_match_single_domain_runs(cuda_device):
         assert t == t1
         for a, b in zip(st, single):
             assert torch.equal(a, b)
-        assert led["volume"] == pytest.approx(led1["volume"], rel=1e-12)
+        # Same states bit for bit; the volumes are summed in a different order
+        # (float partials per 32-row batch in the paired kernel), so they agree
+        # to float64 rounding of float partial sums.
+        assert led["volume"] == pytest.approx(led1["volume"], rel=1e-7)
         assert ledger_error(led) < 1e-6
         times.add(round(t - t0, 6))
     assert len(times) > 1  # members advanced with their own CFL dt
