@@ -34,6 +34,21 @@ struct AdjConsts {
     float g, half_g, dry, eps, dx, dy;
 };
 
+// The reverse step needs derivative values to float accuracy, not the forward's
+// rounding: approximate division, square root and power (a few ulp) keep it cheap.
+__device__ __forceinline__ float adiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float asqrt(float a) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+__device__ __forceinline__ float apow(float x, float e) {  // x > 0
+    float l, r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(x));
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l * e));
+    return r;
+}
+
 struct FaceIn {
     float h, hu, hv, z;
     bool act;
@@ -58,13 +73,13 @@ __device__ void adj_face_fwd(FaceIn lo, FaceIn hi, const AdjConsts& k, float F[3
     }
     const float zf = fmaxf(L.z, R.z);
     const float HL = fmaxf(L.h + L.z - zf, 0.f), HR = fmaxf(R.h + R.z - zf, 0.f);
-    const float uL = L.h > k.dry ? L.hu / L.h : 0.f, vL = L.h > k.dry ? L.hv / L.h : 0.f;
-    const float uR = R.h > k.dry ? R.hu / R.h : 0.f, vR = R.h > k.dry ? R.hv / R.h : 0.f;
+    const float uL = L.h > k.dry ? adiv(L.hu, L.h) : 0.f, vL = L.h > k.dry ? adiv(L.hv, L.h) : 0.f;
+    const float uR = R.h > k.dry ? adiv(R.hu, R.h) : 0.f, vR = R.h > k.dry ? adiv(R.hv, R.h) : 0.f;
     const float XL = HL * uL, YL = HL * vL, XR = HR * uR, YR = HR * vR;
     const float nL = AXIS == 1 ? XL : YL, nR = AXIS == 1 ? XR : YR;
-    const float unL = HL > k.dry ? nL / HL : 0.f, unR = HR > k.dry ? nR / HR : 0.f;
-    const float tL = HL > k.dry ? YL / HL : 0.f, tR = HR > k.dry ? YR / HR : 0.f;
-    const float cL = sqrtf(k.g * HL), cR = sqrtf(k.g * HR);
+    const float unL = HL > k.dry ? adiv(nL, HL) : 0.f, unR = HR > k.dry ? adiv(nR, HR) : 0.f;
+    const float tL = HL > k.dry ? adiv(YL, HL) : 0.f, tR = HR > k.dry ? adiv(YR, HR) : 0.f;
+    const float cL = asqrt(k.g * HL), cR = asqrt(k.g * HR);
     const float sL = fminf(unL - cL, unR - cR), sR = fmaxf(unL + cL, unR + cR);
     const float pL = k.half_g * HL * HL, pR = k.half_g * HR * HR;
     float fL[3], fR[3];
@@ -79,7 +94,7 @@ __device__ void adj_face_fwd(FaceIn lo, FaceIn hi, const AdjConsts& k, float F[3
     const float spread = sR - sL;
     const float den = spread > k.eps ? spread : 1.f;
     for (int q = 0; q < 3; ++q) {
-        const float m = (sR * fL[q] - sL * fR[q] + sL * sR * (UR[q] - UL[q])) / den;
+        const float m = adiv(sR * fL[q] - sL * fR[q] + sL * sR * (UR[q] - UL[q]), den);
         F[q] = sL >= 0.f ? fL[q] : (sR <= 0.f ? fR[q] : m);
     }
     clo = k.half_g * (L.h * L.h - HL * HL);
@@ -108,14 +123,14 @@ __device__ void adj_face_vjp(FaceIn lo, FaceIn hi, const AdjConsts& k, const flo
     const float aL = L.h + L.z - zf, aR = R.h + R.z - zf;
     const float HL = fmaxf(aL, 0.f), HR = fmaxf(aR, 0.f);
     const bool dL = L.h > k.dry, dR = R.h > k.dry;
-    const float uL = dL ? L.hu / L.h : 0.f, vL = dL ? L.hv / L.h : 0.f;
-    const float uR = dR ? R.hu / R.h : 0.f, vR = dR ? R.hv / R.h : 0.f;
+    const float uL = dL ? adiv(L.hu, L.h) : 0.f, vL = dL ? adiv(L.hv, L.h) : 0.f;
+    const float uR = dR ? adiv(R.hu, R.h) : 0.f, vR = dR ? adiv(R.hv, R.h) : 0.f;
     const float XL = HL * uL, YL = HL * vL, XR = HR * uR, YR = HR * vR;
     const float nL = AXIS == 1 ? XL : YL, nR = AXIS == 1 ? XR : YR;
     const bool wL = HL > k.dry, wR = HR > k.dry;
-    const float unL = wL ? nL / HL : 0.f, unR = wR ? nR / HR : 0.f;
-    const float tL = wL ? YL / HL : 0.f, tR = wR ? YR / HR : 0.f;
-    const float cL = sqrtf(k.g * HL), cR = sqrtf(k.g * HR);
+    const float unL = wL ? adiv(nL, HL) : 0.f, unR = wR ? adiv(nR, HR) : 0.f;
+    const float tL = wL ? adiv(YL, HL) : 0.f, tR = wR ? adiv(YR, HR) : 0.f;
+    const float cL = asqrt(k.g * HL), cR = asqrt(k.g * HR);
     const float aminL = unL - cL, aminR = unR - cR, amaxL = unL + cL, amaxR = unR + cR;
     const float sL = fminf(aminL, aminR), sR = fmaxf(amaxL, amaxR);
     const float pL = k.half_g * HL * HL, pR = k.half_g * HR * HR;
@@ -144,8 +159,8 @@ __device__ void adj_face_vjp(FaceIn lo, FaceIn hi, const AdjConsts& k, const flo
         float lden = 0.f;
         for (int q = 0; q < 3; ++q) {
             const float dU = UR[q] - UL[q];
-            const float m = (sR * fL[q] - sL * fR[q] + sL * sR * dU) / den;
-            const float lN = lF[q] / den;
+            const float m = adiv(sR * fL[q] - sL * fR[q] + sL * sR * dU, den);
+            const float lN = adiv(lF[q], den);
             lden -= m * lN;
             lsR += (fL[q] + sL * dU) * lN;
             lsL += (-fR[q] + sR * dU) * lN;
@@ -189,24 +204,24 @@ __device__ void adj_face_vjp(FaceIn lo, FaceIn hi, const AdjConsts& k, const flo
     float lcL = 0.f, lcR = 0.f;
     if (aminL <= aminR) { lunL += lsL; lcL -= lsL; } else { lunR += lsL; lcR -= lsL; }
     if (amaxL >= amaxR) { lunL += lsR; lcL += lsR; } else { lunR += lsR; lcR += lsR; }
-    if (cL > 0.f) lHL += 0.5f * k.g / cL * lcL;
-    if (cR > 0.f) lHR += 0.5f * k.g / cR * lcR;
+    if (cL > 0.f) lHL += adiv(0.5f * k.g, cL) * lcL;
+    if (cR > 0.f) lHR += adiv(0.5f * k.g, cR) * lcR;
     // un = n / H, t = Y / H (for H > dry)
     float lnL = 0.f, lnR = 0.f;
     if (wL) {
-        lnL += lunL / HL;
-        lHL -= unL / HL * lunL;
+        lnL += adiv(lunL, HL);
+        lHL -= adiv(unL, HL) * lunL;
         if (AXIS == 1) {
-            lYL += ltL / HL;
-            lHL -= tL / HL * ltL;
+            lYL += adiv(ltL, HL);
+            lHL -= adiv(tL, HL) * ltL;
         }
     }
     if (wR) {
-        lnR += lunR / HR;
-        lHR -= unR / HR * lunR;
+        lnR += adiv(lunR, HR);
+        lHR -= adiv(unR, HR) * lunR;
         if (AXIS == 1) {
-            lYR += ltR / HR;
-            lHR -= tR / HR * ltR;
+            lYR += adiv(ltR, HR);
+            lHR -= adiv(tR, HR) * ltR;
         }
     }
     if (AXIS == 1) { lXL += lnL; lXR += lnR; } else { lYL += lnL; lYR += lnR; }
@@ -220,14 +235,14 @@ __device__ void adj_face_vjp(FaceIn lo, FaceIn hi, const AdjConsts& k, const flo
     // u = hu / h, v = hv / h (for h > dry)
     float gL[3] = {lLh, 0.f, 0.f}, gR[3] = {lRh, 0.f, 0.f};
     if (dL) {
-        gL[1] = luL / L.h;
-        gL[2] = lvL / L.h;
-        gL[0] -= (uL * luL + vL * lvL) / L.h;
+        gL[1] = adiv(luL, L.h);
+        gL[2] = adiv(lvL, L.h);
+        gL[0] -= adiv(uL * luL + vL * lvL, L.h);
     }
     if (dR) {
-        gR[1] = luR / R.h;
-        gR[2] = lvR / R.h;
-        gR[0] -= (uR * luR + vR * lvR) / R.h;
+        gR[1] = adiv(luR, R.h);
+        gR[2] = adiv(lvR, R.h);
+        gR[0] -= adiv(uR * luR + vR * lvR, R.h);
     }
     // undo the wall mirroring: the mirrored side's gradient belongs to the active cell
     const int nq = AXIS == 1 ? 1 : 2;
@@ -255,6 +270,7 @@ struct AdjLaunch {
     StepScalars s;       // float32 dt, dt*rate (scaled), dt*g
     float dt_rate;       // float32 dt * rate(t) before the rain scale
     AdjConsts k;
+    float rdx, rdy;      // 1/dx, 1/dy
 };
 
 __device__ __forceinline__ Cell adj_load(const DomainDev& d, const StateView& s, int r, int c) {
@@ -281,7 +297,7 @@ __device__ void adj_cell_update(const AdjLaunch& p, int r, int c, float upd[3]) 
         const float xr = Fl[q] + (q == 1 ? cl_hi : 0.f);
         const float yb = Ft[q] + (q == 2 ? ct_lo : 0.f);
         const float yt = Fb[q] + (q == 2 ? cb_hi : 0.f);
-        upd[q] = U[q] - p.s.dt * ((xl - xr) / p.k.dx + (yb - yt) / p.k.dy);
+        upd[q] = U[q] - p.s.dt * ((xl - xr) * p.rdx + (yb - yt) * p.rdy);
     }
 }
 
@@ -304,26 +320,27 @@ __global__ void __launch_bounds__(THREADS) adj_cell_kernel(const AdjLaunch p) {
         const float mult = d.mult ? d.mult[(int64_t)r * d.spitch + c] : 1.f;
         upd[0] += p.s.dt_rain * mult;
         const float h = fmaxf(upd[0], 0.f);
-        const float norm = sqrtf(upd[1] * upd[1] + upd[2] * upd[2]);
+        const float norm = asqrt(upd[1] * upd[1] + upd[2] * upd[2]);
         const float m = fmaxf(h, p.k.dry);
-        const float pw = powf(m, -7.0f / 3.0f);
+        const float pw = apow(m, -7.0f / 3.0f);
         const float n2 = fabsf(nm);
         const float fr = p.s.dt_g * n2 * norm * pw;
         const float den = 1.f + fr;
-        const float qx = upd[1] / den, qy = upd[2] / den;
+        const float rden = adiv(1.f, den);
+        const float qx = upd[1] * rden, qy = upd[2] * rden;
         const bool wet = h > p.k.dry;
         const int64_t li = (int64_t)r * p.lam.pitch + c;
         const float lqx = wet ? p.lam.hu[li] : 0.f, lqy = wet ? p.lam.hv[li] : 0.f;
         float lh = p.lam.h[li];
-        const float lden = -(lqx * qx + lqy * qy) / den;
-        float lu1 = lqx / den, lu2 = lqy / den;
+        const float lden = -(lqx * qx + lqy * qy) * rden;
+        float lu1 = lqx * rden, lu2 = lqy * rden;
         if (norm > 0.f) {
             const float lnorm = lden * p.s.dt_g * n2 * pw;
-            lu1 += lnorm * upd[1] / norm;
-            lu2 += lnorm * upd[2] / norm;
+            lu1 += adiv(lnorm * upd[1], norm);
+            lu2 += adiv(lnorm * upd[2], norm);
         }
         p.grad_n2[(int64_t)r * d.cols + c] += lden * p.s.dt_g * norm * pw;
-        if (h > p.k.dry) lh += lden * fr * (-7.0f / 3.0f) / h;
+        if (h > p.k.dry) lh += adiv(lden * fr * (-7.0f / 3.0f), h);
         const float lu0 = upd[0] > 0.f ? lh : 0.f;
         rain_acc += (double)lu0 * (double)p.dt_rate * (double)mult;
         p.lupd[0][lo] = lu0;
@@ -357,7 +374,7 @@ template <int THREADS>
 __global__ void __launch_bounds__(THREADS) adj_face_kernel(const AdjLaunch p) {
     const DomainDev& d = p.d;
     const int64_t n = (int64_t)d.rows * d.cols;
-    const float ax = p.s.dt / p.k.dx, ay = p.s.dt / p.k.dy;
+    const float ax = p.s.dt * p.rdx, ay = p.s.dt * p.rdy;
     for (int64_t i = (int64_t)blockIdx.x * THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * THREADS) {
         const int r = (int)(i / d.cols), c = (int)(i - (int64_t)r * d.cols);
         float g[3];

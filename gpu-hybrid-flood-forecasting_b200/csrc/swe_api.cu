@@ -973,6 +973,8 @@ int swe_adjoint_step(swe_domain_t d, const float* h, const float* hu, const floa
     al.s.dt_g = (float)dg;
     al.dt_rate = (float)dru;
     al.k = AdjConsts{d->dd.k.g, d->dd.k.half_g, d->dd.k.dry, d->dd.k.eps, d->dd.k.dx, d->dd.k.dy};
+    al.rdx = 1.0f / d->dd.k.dx;
+    al.rdy = 1.0f / d->dd.k.dy;
     const int64_t n = (int64_t)rows * d->dd.cols;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + kThreads - 1) / kThreads, (int64_t)d->sms * 16));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
