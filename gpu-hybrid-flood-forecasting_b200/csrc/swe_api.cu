@@ -1178,6 +1178,32 @@ int swe_network_features(swe_domain_t d, const float* h, const float* hu, const 
     return SWE_OK;
 }
 
+int swe_output_fields(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch,
+                      float* depth, float* x_velocity, float* y_velocity, float* speed, int64_t out_pitch,
+                      void* stream) {
+    if (!d || !depth || !x_velocity || !y_velocity || !speed) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    if (out_pitch < d->dd.cols) return fail(SWE_ERR_INVALID, "output pitch smaller than the column count");
+    SchemaArgs a{};
+    a.rows = d->dd.rows;
+    a.cols = d->dd.cols;
+    a.s = StateView{h, hu, hv, pitch};
+    a.nm = d->nm;
+    a.spitch = d->dd.spitch;
+    a.dry = d->dd.k.dry;
+    a.depth = depth;
+    a.u = x_velocity;
+    a.v = y_velocity;
+    a.speed = speed;
+    a.out_pitch = out_pitch;
+    const int64_t n = (int64_t)a.rows * a.cols;
+    schema_kernel<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)d->sms * 8), 256, 0,
+                    static_cast<cudaStream_t>(stream)>>>(a);
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
 int swe_apply_correction(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch,
                          const void* residual, int32_t residual_bf16, int64_t res_stride_row,
                          int64_t res_stride_col, int64_t res_stride_channel, int32_t res_channels,

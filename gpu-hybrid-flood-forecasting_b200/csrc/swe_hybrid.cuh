@@ -157,4 +157,36 @@ __global__ void correction_apply_kernel(const CorrectionArgs a) {
     }
 }
 
+// Output schema of a state (conserved_to_xarray, structured_io.py:160-209):
+// depth, x/y velocity (momentum / depth where depth > dry, else 0) and speed
+// (hypot, evaluated in double and rounded once as float32 hypot is), each NaN
+// off the domain mask.  IEEE division, so the fields equal NumPy's bit for bit.
+struct SchemaArgs {
+    int rows, cols;
+    StateView s;
+    const float* nm;
+    int64_t spitch;
+    float dry;
+    float *depth, *u, *v, *speed;
+    int64_t out_pitch;
+};
+
+__global__ void schema_kernel(const SchemaArgs a) {
+    const int64_t n = (int64_t)a.rows * a.cols;
+    const float nan = __int_as_float(0x7fc00000);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / a.cols), c = (int)(i - (int64_t)r * a.cols);
+        const int64_t so = (int64_t)r * a.s.pitch + c, oo = (int64_t)r * a.out_pitch + c;
+        const bool act = active(a.nm[(int64_t)r * a.spitch + c]);
+        const float h = a.s.h[so];
+        const bool wet = h > a.dry;
+        const float u = wet ? __fdiv_rn(a.s.hu[so], h) : 0.f;
+        const float v = wet ? __fdiv_rn(a.s.hv[so], h) : 0.f;
+        a.depth[oo] = act ? h : nan;
+        a.u[oo] = act ? u : nan;
+        a.v[oo] = act ? v : nan;
+        a.speed[oo] = act ? ExactMath::hypot(u, v) : nan;
+    }
+}
+
 }  // namespace swe

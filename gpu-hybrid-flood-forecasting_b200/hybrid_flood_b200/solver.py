@@ -209,6 +209,7 @@ class B200ShallowWaterSolver:
             arithmetic=arithmetic, device=self.device,
         )
         self.domain_mask = torch.from_numpy(mask_h).to(self.device)
+        self.bed = bed_h  # host copy (the output schema's elevation)
         self.shape = tuple(shape)
 
     def __del__(self):

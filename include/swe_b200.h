@@ -208,6 +208,15 @@ int swe_network_features(swe_domain_t d, const float *h, const float *hu, const 
                          const float *terrain, const float *roughness, void *out, int32_t out_bf16,
                          void *stream);
 
+/* Output fields of a state in the common forecast schema (conserved_to_xarray,
+ * src/hybrid_flood/structured_io.py:160-209): depth, x_velocity and y_velocity
+ * (momentum / depth where depth > dry_tolerance, else 0) and velocity (their
+ * hypot), each NaN off the domain mask.  Outputs are four device float32 planes
+ * of pitch out_pitch; values equal the reference's NumPy arrays bit for bit. */
+int swe_output_fields(swe_domain_t d, const float *h, const float *hu, const float *hv, int64_t pitch,
+                      float *depth, float *x_velocity, float *y_velocity, float *speed, int64_t out_pitch,
+                      void *stream);
+
 /* Volume-preserving residual correction (apply_residual_correction,
  * hybrid/coupled_forecast.py:82-120), with the clip of :199-200 fused in:
  * res = clip(residual, -clip_limits, clip_limits) per channel (host

@@ -128,3 +128,18 @@ def test_oracle_features_layouts():
     g = HN.state5_features(h, hu, hv, t, mask, 20.0, [0] * 5, [2] * 5)
     assert g.shape == (1, *mask.shape, 5)
     np.testing.assert_array_equal(g[0, ..., 4], np.where(mask, np.float32(10.0), 0))
+
+
+def test_output_oracle_schema_fields():
+    """structured_io.py:160-209: velocities only where depth > dry, NaN off the mask."""
+    from oracle import output_numpy as ON
+
+    _, mask, h, hu, hv = _grid(4)
+    d, u, v, s = ON.conserved_fields(h, hu, hv, mask, 1e-4)
+    assert np.isnan(d[~mask]).all() and np.isnan(s[~mask]).all()
+    wet = mask & (h > 1e-4)
+    np.testing.assert_array_equal(u[wet], (hu[wet] / h[wet]).astype(np.float32))
+    assert not u[mask & ~wet].any()
+    np.testing.assert_array_equal(s[mask], np.hypot(u[mask], v[mask]).astype(np.float32))
+    stack = ON.conserved_fields(np.stack([h, h]), np.stack([hu, hu]), np.stack([hv, hv]), mask, 1e-4)
+    np.testing.assert_array_equal(stack[0][1], d)
