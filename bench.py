@@ -291,7 +291,7 @@ def _adjoint(args, dev):
     f_ms = ev[0].elapsed_time(ev[1])
     fb_ms = ev[2].elapsed_time(ev[3])
     return {"workload": "512x512 dx=2m tilted plane + bumps, log-normal n (median 0.03, sigma_log 0.3, "
-                        "9-cell smoothing), 16 gauges every 10 steps, 2000 fixed-dt steps, checkpoint/50",
+                        f"9-cell smoothing), 16 gauges every 10 steps, {steps} fixed-dt steps, checkpoint/50",
             "steps": steps, "forward_ms": f_ms, "forward_adjoint_ms": fb_ms, "ratio": fb_ms / f_ms,
             "loss": float(loss.detach()), "grad_n_norm": float(n_t.grad.norm()), "grad_rain_scale": float(s_t.grad)}
 
