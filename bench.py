@@ -50,6 +50,11 @@ sys.path.insert(0, str(REPO))
 
 METRIC = "cell-updates/s (plain single-domain step, 2048x2048 urban)"
 BYTES_PER_CELL = 32  # h, hu, hv, bed, n^2 read (20 B) + h, hu, hv written (12 B)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fast-arithmetic
+# step_kernel_pair launch on the default 2048x2048 workload, per cell-update, from an
+# ncu --set full capture of that launch (103.8 MB read + 12.8 MB written): reported as
+# roofline.traffic for that configuration only.
+NCU_TRAFFIC_PER_CELL = (103.774976e6 + 12.771328e6) / 4194304
 
 
 def _args():
@@ -538,7 +543,10 @@ def run_b200(args, rank: int, world: int):
                    "l2": "per-step working set 134 MB > 126 MB L2; no flush",
                    "simulated_window_s": window, "spinup_steps": args.spinup},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": (NCU_TRAFFIC_PER_CELL * cells
+                                 if (args.rows, args.cols, args.arith) == (2048, 2048, "fast") else None),
+                     "traffic_unit": "bytes per launch (ncu capture of the same launch)",
                      "kernel": "step_kernel (fused step + CFL + ledger)",
                      "bytes_per_cell": BYTES_PER_CELL, "peak_kind": peak_kind,
                      "kernel_ms_per_launch": per_launch_ms},
