@@ -261,6 +261,7 @@ __device__ void adj_face_vjp(FaceIn lo, FaceIn hi, const AdjConsts& k, const flo
 struct AdjLaunch {
     DomainDev d;
     StateView in;        // U_k
+    StateView next;      // U_{k+1} when known (h == nullptr otherwise)
     StateView lam;       // dL/dU_{k+1}
     StateOut lam_out;    // dL/dU_k
     float* lupd[3];      // scratch: dL/d(upd) planes, pitch lpitch
@@ -301,7 +302,29 @@ __device__ void adj_cell_update(const AdjLaunch& p, int r, int c, float upd[3]) 
     }
 }
 
-template <int THREADS>
+// The cell update before the pointwise part, rebuilt from the step's own output
+// U_{k+1} = (h1, hu1, hv1) of an active cell instead of from its four faces.
+// The momenta invert the semi-implicit friction: with a = dt g n^2 max(h,dry)^(-7/3),
+// q = upd/(1 + a|upd|) gives upd = q/(1 - a|q|).  Returns false (rebuild from the
+// faces instead) where that inversion loses precision (a|q| > 0.999, i.e. friction
+// dividing the momentum by more than 1000).  For dry or clipped cells only the
+// depth part is needed: the momentum outputs are zero and carry no gradient.
+__device__ __forceinline__ bool adj_upd_from_next(const AdjLaunch& p, int r, int c, float n2, float upd[3]) {
+    const int64_t o = (int64_t)r * p.next.pitch + c;
+    const float h1 = p.next.h[o];
+    upd[0] = h1;  // only the sign of upd0 + rain and h itself are used below
+    upd[1] = upd[2] = 0.f;
+    if (!(h1 > p.k.dry)) return true;
+    const float q1 = p.next.hu[o], q2 = p.next.hv[o];
+    const float aq = p.s.dt_g * n2 * apow(h1, -7.0f / 3.0f) * asqrt(q1 * q1 + q2 * q2);
+    if (!(aq <= 0.999f)) return false;
+    const float den = adiv(1.f, 1.f - aq);
+    upd[1] = q1 * den;
+    upd[2] = q2 * den;
+    return true;
+}
+
+template <int THREADS, bool NEXT>
 __global__ void __launch_bounds__(THREADS) adj_cell_kernel(const AdjLaunch p) {
     const DomainDev& d = p.d;
     const int64_t n = (int64_t)d.rows * d.cols;
@@ -315,10 +338,13 @@ __global__ void __launch_bounds__(THREADS) adj_cell_kernel(const AdjLaunch p) {
             p.lupd[0][lo] = p.lupd[1][lo] = p.lupd[2][lo] = 0.f;
             continue;
         }
-        float upd[3];
-        adj_cell_update(p, r, c, upd);
         const float mult = d.mult ? d.mult[(int64_t)r * d.spitch + c] : 1.f;
-        upd[0] += p.s.dt_rain * mult;
+        float upd[3];
+        // upd[0] below is the depth after the rain (before the clip).
+        if (!(NEXT && adj_upd_from_next(p, r, c, fabsf(nm), upd))) {
+            adj_cell_update(p, r, c, upd);
+            upd[0] += p.s.dt_rain * mult;
+        }
         const float h = fmaxf(upd[0], 0.f);
         const float norm = asqrt(upd[1] * upd[1] + upd[2] * upd[2]);
         const float m = fmaxf(h, p.k.dry);

@@ -111,6 +111,7 @@ struct swe_domain {
     float* lupd[3] = {nullptr, nullptr, nullptr};  // adjoint scratch
     int64_t lpitch = 0;
     double* times64_dev = nullptr;  // float64 targets of advance_to
+    float* next_scratch = nullptr;  // rollout backward: the output of a segment's last step
     double* corr_sums = nullptr;    // volume sums of the residual correction
     float* corr_prov = nullptr;     // provisional-depth plane of the correction
     unsigned* done_counter = nullptr;  // set by an ensemble: shared completion counter
@@ -399,6 +400,7 @@ void free_domain(swe_domain* d) {
     cudaFree(d->times_dev);
     for (int q = 0; q < 3; ++q) cudaFree(d->lupd[q]);
     cudaFree(d->times64_dev);
+    cudaFree(d->next_scratch);
     cudaFree(d->corr_sums);
     cudaFree(d->corr_prov);
     for (int i = 0; i < 2; ++i) {
@@ -939,17 +941,14 @@ int swe_domain_set_manning(swe_domain_t d, const float* manning_n, int32_t on_ho
     return SWE_OK;
 }
 
-int swe_adjoint_step(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch,
-                     const float* lam_h, const float* lam_hu, const float* lam_hv, int64_t lam_pitch,
-                     float* lam_h_out, float* lam_hu_out, float* lam_hv_out, int64_t out_pitch,
-                     float* grad_n2, double* grad_rain_scale, double dt, double time_s, void* stream) {
-    if (!d || !grad_n2 || !grad_rain_scale) return fail(SWE_ERR_INVALID, "null argument");
-    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
-    if (rc) return rc;
-    rc = check_state_ptrs(lam_h, lam_hu, lam_hv, lam_pitch, d->dd.cols);
-    if (rc) return rc;
-    rc = check_state_ptrs(lam_h_out, lam_hu_out, lam_hv_out, out_pitch, d->dd.cols);
-    if (rc) return rc;
+namespace {
+
+// One reverse step; `next` (U_{k+1}, or null) lets the cell part skip the face recompute.
+int adjoint_step_impl(swe_domain* d, const float* h, const float* hu, const float* hv, int64_t pitch,
+                      const float* next, int64_t next_pitch, int64_t next_plane,
+                      const float* lam_h, const float* lam_hu, const float* lam_hv, int64_t lam_pitch,
+                      float* lam_h_out, float* lam_hu_out, float* lam_hv_out, int64_t out_pitch,
+                      float* grad_n2, double* grad_rain_scale, double dt, double time_s, cudaStream_t st) {
     const int rows = d->dd.rows;
     if (!d->lupd[0]) {
         d->lpitch = round_up(d->dd.cols, 128);
@@ -959,6 +958,8 @@ int swe_adjoint_step(swe_domain_t d, const float* h, const float* hu, const floa
     AdjLaunch al{};
     al.d = d->dd;
     al.in = StateView{h, hu, hv, pitch};
+    al.next = next ? StateView{next, next + next_plane, next + 2 * next_plane, next_pitch}
+                   : StateView{nullptr, nullptr, nullptr, 0};
     al.lam = StateView{lam_h, lam_hu, lam_hv, lam_pitch};
     al.lam_out = StateOut{lam_h_out, lam_hu_out, lam_hv_out, out_pitch};
     for (int q = 0; q < 3; ++q) al.lupd[q] = d->lupd[q];
@@ -977,11 +978,31 @@ int swe_adjoint_step(swe_domain_t d, const float* h, const float* hu, const floa
     al.rdy = 1.0f / d->dd.k.dy;
     const int64_t n = (int64_t)rows * d->dd.cols;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + kThreads - 1) / kThreads, (int64_t)d->sms * 16));
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    adj_cell_kernel<kThreads><<<blocks, kThreads, 0, st>>>(al);
+    if (next)
+        adj_cell_kernel<kThreads, true><<<blocks, kThreads, 0, st>>>(al);
+    else
+        adj_cell_kernel<kThreads, false><<<blocks, kThreads, 0, st>>>(al);
     adj_face_kernel<kThreads><<<blocks, kThreads, 0, st>>>(al);
     SWE_CK(cudaGetLastError());
     return SWE_OK;
+}
+
+}  // namespace
+
+int swe_adjoint_step(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch,
+                     const float* lam_h, const float* lam_hu, const float* lam_hv, int64_t lam_pitch,
+                     float* lam_h_out, float* lam_hu_out, float* lam_hv_out, int64_t out_pitch,
+                     float* grad_n2, double* grad_rain_scale, double dt, double time_s, void* stream) {
+    if (!d || !grad_n2 || !grad_rain_scale) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    rc = check_state_ptrs(lam_h, lam_hu, lam_hv, lam_pitch, d->dd.cols);
+    if (rc) return rc;
+    rc = check_state_ptrs(lam_h_out, lam_hu_out, lam_hv_out, out_pitch, d->dd.cols);
+    if (rc) return rc;
+    return adjoint_step_impl(d, h, hu, hv, pitch, nullptr, 0, 0, lam_h, lam_hu, lam_hv, lam_pitch, lam_h_out,
+                             lam_hu_out, lam_hv_out, out_pitch, grad_n2, grad_rain_scale, dt, time_s,
+                             static_cast<cudaStream_t>(stream));
 }
 
 int swe_step(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch_in,
@@ -1309,6 +1330,7 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int rows = d->dd.rows, cols = d->dd.cols;
     const int64_t plane = (int64_t)rows * cols;
+    if (!d->next_scratch) SWE_CK(cudaMalloc(&d->next_scratch, sizeof(float) * 3 * (size_t)plane));
     float* lam[3] = {lam_h, lam_hu, lam_hv};
     if (!lam_in)
         for (int f = 0; f < 3; ++f)
@@ -1327,6 +1349,15 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
                           dts ? dts[k] : dt, step_time(k, dt, t0, dts), stream);
             if (rc) return rc;
         }
+        // U_{k1}, the output of the segment's last step, so that every reverse step
+        // can rebuild its cell updates from its own output.
+        {
+            const float* a = seg + (int64_t)(k1 - 1 - k0) * 3 * plane;
+            rc = swe_step(d, a, a + plane, a + 2 * plane, cols, d->next_scratch, d->next_scratch + plane,
+                          d->next_scratch + 2 * plane, cols, dts ? dts[k1 - 1] : dt, step_time(k1 - 1, dt, t0, dts),
+                          stream);
+            if (rc) return rc;
+        }
         for (int k = k1 - 1; k >= k0; --k) {
             if (n_gauges > 0 && (k + 1) % obs_every == 0) {
                 gauge_inject_kernel<<<(n_gauges + 127) / 128, 128, 0, st>>>(
@@ -1334,9 +1365,10 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
                     grad_obs + (int64_t)((k + 1) / obs_every - 1) * n_gauges);
             }
             const float* a = seg + (int64_t)(k - k0) * 3 * plane;
-            rc = swe_adjoint_step(d, a, a + plane, a + 2 * plane, cols, lam_h, lam_hu, lam_hv, lam_pitch,
-                                  lam_h, lam_hu, lam_hv, lam_pitch, grad_n2, grad_rain_scale,
-                                  dts ? dts[k] : dt, step_time(k, dt, t0, dts), stream);
+            const float* nx = k + 1 < k1 ? seg + (int64_t)(k + 1 - k0) * 3 * plane : d->next_scratch;
+            rc = adjoint_step_impl(d, a, a + plane, a + 2 * plane, cols, nx, cols, plane, lam_h, lam_hu, lam_hv,
+                                   lam_pitch, lam_h, lam_hu, lam_hv, lam_pitch, grad_n2, grad_rain_scale,
+                                   dts ? dts[k] : dt, step_time(k, dt, t0, dts), st);
             if (rc) return rc;
         }
     }

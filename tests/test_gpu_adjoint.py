@@ -171,3 +171,53 @@ def test_step_function_autograd_chain_matches_finite_differences(cuda_device):
     fd_n = (J(U, n64 + eps * dn) - J(U, n64 - eps * dn)) / (2 * eps)
     ad_n = float((n_t.grad.cpu().numpy().astype(np.float64) * dn).sum())
     assert ad_n == pytest.approx(fd_n, rel=5e-3, abs=1e-12)
+
+
+def test_rollout_backward_matches_stepwise_reverse(cuda_device):
+    """The rollout's reverse steps rebuild each cell update from the step's own output
+    (or from the faces where strong friction makes that inexact); the standalone
+    reverse step always rebuilds it from the faces.  Both must give the same
+    gradients, here on a shallow, rough case where both branches occur."""
+    from hybrid_flood_b200.adjoint import adjoint_step, set_manning
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver, SWEState, _ptr, _stream
+
+    w, mask, n, kw, _, _, _ = _case(32, 48, (0, 1, 0, 0), True, seed=8)
+    rng = np.random.default_rng(8)
+    n = rng.uniform(0.03, 0.3, w.shape).astype(np.float32)
+    depth = rng.uniform(0.002, 0.3, w.shape).astype(np.float32)
+    s = B200ShallowWaterSolver(w.bed, n, mask, **kw)
+    set_manning(s, n)
+    st = s.initial_state(depth_m=depth, x_velocity_m_s=0.2, y_velocity_m_s=-0.1)
+    steps, dt, t0, every = 12, 0.05, 5.0, 4
+    H, W = w.shape
+    dev = cuda_device
+    # forward, keeping every state
+    states = [SWEState(*(a.clone() for a in st))]
+    for k in range(steps):
+        states.append(s.step(states[-1], dt, t0 + k * dt))
+    g_final = [torch.tensor(rng.normal(0, 1, w.shape), dtype=torch.float32, device=dev) for _ in range(3)]
+    # stepwise reverse (faces recomputed in every reverse step)
+    lam = SWEState(*(g.clone() for g in g_final))
+    gn2_a = torch.zeros((H, W), device=dev)
+    gr_a = torch.zeros(1, dtype=torch.float64, device=dev)
+    t = [t0]
+    for k in range(steps - 1):
+        t.append(t[-1] + dt)
+    for k in range(steps - 1, -1, -1):
+        lam = adjoint_step(s, states[k], lam, dt, t[k], gn2_a, gr_a)
+    # the rollout's reverse pass from one checkpoint, final-state gradient on entry
+    ckpt = torch.stack(list(states[0]))[None].contiguous()
+    seg = torch.empty((steps, 3, H, W), device=dev)
+    lb = [g.clone() for g in g_final]
+    gn2_b = torch.zeros((H, W), device=dev)
+    gr_b = torch.zeros(1, dtype=torch.float64, device=dev)
+    with torch.cuda.device(dev):
+        rc = s._lib.swe_rollout_backward(s._handle, _ptr(ckpt), steps, steps, dt, t0, None, None, 0, 1, None,
+                                         _ptr(lb[0]), _ptr(lb[1]), _ptr(lb[2]), W, 1, _ptr(gn2_b), _ptr(gr_b),
+                                         _ptr(seg), _stream(dev))
+    assert rc == 0
+    for a, b in zip(lam, lb):
+        a, b = a.cpu().numpy().astype(np.float64), b.cpu().numpy().astype(np.float64)
+        assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(a)
+    ga, gb = gn2_a.cpu().numpy().astype(np.float64), gn2_b.cpu().numpy().astype(np.float64)
+    assert np.linalg.norm(ga - gb) <= 1e-3 * np.linalg.norm(ga)
