@@ -336,8 +336,10 @@ def _hybrid(args, dev):
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
+    tm: dict = {}
+    ens.set_timing(True)
     e0.record(stream)
-    traj, steps = run_coupled_ensemble(ens, states, net, hi, times, **kw)
+    traj, steps = run_coupled_ensemble(ens, states, net, hi, times, **kw, timings=tm)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     total_ms = e0.elapsed_time(e1)
@@ -361,6 +363,8 @@ def _hybrid(args, dev):
             "ms_per_interval": total_ms / args.hybrid_intervals, "physics_steps_mean": float(steps.mean()),
             "physics_steps_max": int(steps.max()), "corrector_ms_per_interval": net_ms,
             "corrector_share": net_ms * args.hybrid_intervals / total_ms,
+            "physics_ms_per_interval": tm.get("physics_ms", 0.0) / args.hybrid_intervals,
+            "physics_cell_updates_per_s": phys_updates / (tm["physics_ms"] / 1e3) if tm.get("physics_ms") else None,
             "cell_updates_per_s": phys_updates / (total_ms / 1e3), "finite": finite}
 
 

@@ -87,7 +87,7 @@ class B200Ensemble:
         self.shapes = [tuple(np.asarray(m["bed"]).shape) for m in members]
         self.masks = [torch.from_numpy(np.asarray(m["domain_mask"], dtype=bool)).to(self.device) for m in members]
         self.arithmetic = arithmetic
-        self.rows_per_warp = 16
+        self.rows_per_warp = 64
         self.dry_tolerances = [float(m.get("dry_tolerance_m", 1.0e-4)) for m in members]
         self.beds = [np.asarray(m["bed"], dtype=np.float32) for m in members]
 

@@ -331,7 +331,7 @@ def ensemble_domains(ensemble) -> list[_Domain]:
 def run_coupled_ensemble(ensemble, initial_states, model, hybrid_inputs: HybridInputs, output_times_s, *,
                          max_substeps_per_interval: int, correction_relaxation: float = 0.05,
                          correction_clip_sigma: float = 5.0, feature_layout: str = "state5",
-                         keep_states: bool = True):
+                         keep_states: bool = True, timings: dict | None = None):
     """The coupled rollout of every member of an ensemble, the corrector batched over members.
 
     All members must share one grid shape (the corrector runs on one
@@ -340,7 +340,9 @@ def run_coupled_ensemble(ensemble, initial_states, model, hybrid_inputs: HybridI
     persistent multi-member kernel), one batched corrector call, and the
     correction of each member.  Returns ``(states, physics_steps_per_member)``
     where ``states[m]`` is that member's ``[T, rows, cols]`` trajectory (or its
-    final state only when ``keep_states`` is false).
+    final state only when ``keep_states`` is false).  With ``timings`` (a dict)
+    and ensemble timing on (``set_timing``), the device time of the physics
+    advances is summed into ``timings["physics_ms"]``.
     """
     if max_substeps_per_interval < 1:
         raise ValueError("At least one physics substep per correction interval is required.")
@@ -380,6 +382,10 @@ def run_coupled_ensemble(ensemble, initial_states, model, hybrid_inputs: HybridI
                 network_features(doms[m], cur[m], his[m], times[k - 1], layout=feature_layout, dtype=fdtype,
                                  out=feats[m], _planes=planes[m])
             res = ensemble.advance_to_(cur, times[k - 1], times[k], int(max_substeps_per_interval))
+            if timings is not None:
+                ms, launches = ensemble.last_step_time()
+                timings["physics_ms"] = timings.get("physics_ms", 0.0) + ms
+                timings["physics_launches"] = timings.get("physics_launches", 0) + launches
             for m, (t, n, _) in enumerate(res):
                 steps[m] += n
                 if not t >= times[k] - 1.0e-6:

@@ -24,7 +24,7 @@ import torch.nn.functional as F
 from torch import nn
 
 _ACTIVATIONS = {
-    "relu": lambda: nn.ReLU(),
+    "relu": lambda: nn.ReLU(inplace=True),  # in place: each convolution's output is not needed again
     "gelu": lambda: nn.GELU(approximate="tanh"),  # Flax's default GELU is the tanh form
     "silu": lambda: nn.SiLU(),
     "tanh": lambda: nn.Tanh(),

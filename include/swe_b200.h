@@ -244,7 +244,7 @@ int swe_ensemble_create(const swe_domain_desc *descs, int32_t n_members, swe_ens
 int swe_ensemble_destroy(swe_ensemble_t e);
 int swe_ensemble_size(swe_ensemble_t e);
 
-/* Rows each warp marches per work item (the tuning knob of the work list). */
+/* Rows each warp marches per work item (the tuning knob of the work list; default 64). */
 int swe_ensemble_set_rows_per_warp(swe_ensemble_t e, int32_t rows_per_warp);
 
 /* Advance every member IN PLACE by n_steps of its own CFL dt, starting at
