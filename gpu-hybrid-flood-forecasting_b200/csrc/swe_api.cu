@@ -21,6 +21,7 @@
 #include "swe_step_pair.cuh"
 #include "swe_adjoint.cuh"
 #include "swe_hybrid.cuh"
+#include "swe_nn.cuh"
 
 using namespace swe;
 
@@ -1221,6 +1222,32 @@ int swe_output_fields(swe_domain_t d, const float* h, const float* hu, const flo
     const int64_t n = (int64_t)a.rows * a.cols;
     schema_kernel<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)d->sms * 8), 256, 0,
                     static_cast<cudaStream_t>(stream)>>>(a);
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
+int swe_bias_act_nhwc(void* y, int64_t n, int32_t channels, const float* bias, int32_t relu, int32_t bf16,
+                      int32_t device, void* stream) {
+    if (!y || !bias || n < 0 || channels < 1 || n % channels) return fail(SWE_ERR_INVALID, "bad bias/activation arguments");
+    if (n == 0) return SWE_OK;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool vec = bf16 && channels % 8 == 0 && reinterpret_cast<uintptr_t>(y) % 16 == 0;
+    const int64_t work = vec ? n / 8 : n;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)sms * 16));
+    auto* yb = static_cast<__nv_bfloat16*>(y);
+    auto* yf = static_cast<float*>(y);
+    if (vec) {
+        if (relu) bias_act_bf16x8_kernel<true><<<blocks, 256, 0, st>>>(yb, work, channels, bias);
+        else bias_act_bf16x8_kernel<false><<<blocks, 256, 0, st>>>(yb, work, channels, bias);
+    } else if (bf16) {
+        if (relu) bias_act_scalar_kernel<__nv_bfloat16, true><<<blocks, 256, 0, st>>>(yb, n, channels, bias);
+        else bias_act_scalar_kernel<__nv_bfloat16, false><<<blocks, 256, 0, st>>>(yb, n, channels, bias);
+    } else {
+        if (relu) bias_act_scalar_kernel<float, true><<<blocks, 256, 0, st>>>(yf, n, channels, bias);
+        else bias_act_scalar_kernel<float, false><<<blocks, 256, 0, st>>>(yf, n, channels, bias);
+    }
     SWE_CK(cudaGetLastError());
     return SWE_OK;
 }

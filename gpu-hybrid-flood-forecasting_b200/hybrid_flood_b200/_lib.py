@@ -46,6 +46,7 @@ EXPORTS = (
     "swe_network_features",
     "swe_apply_correction",
     "swe_output_fields",
+    "swe_bias_act_nhwc",
     "swe_ensemble_create",
     "swe_ensemble_destroy",
     "swe_ensemble_size",
@@ -146,6 +147,7 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_apply_correction": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _vp, _i32, _i64, _i64, _i64, _i32,
                                                 _vp, _f64, _vp, _vp, _vp, _i64, _vp]),
         "swe_output_fields": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
+        "swe_bias_act_nhwc": (ctypes.c_int, [_vp, _i64, _i32, _vp, _i32, _i32, _i32, _vp]),
         "swe_ensemble_create": (ctypes.c_int, [ctypes.POINTER(DomainDesc), _i32, ctypes.POINTER(_vp)]),
         "swe_ensemble_destroy": (ctypes.c_int, [_vp]),
         "swe_ensemble_size": (ctypes.c_int, [_vp]),

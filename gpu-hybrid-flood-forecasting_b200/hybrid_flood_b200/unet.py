@@ -12,19 +12,68 @@ initialised 1×1 head.  Submodule names equal the reference's so its
 On the B200 the network runs in bfloat16 with ``channels_last`` tensors (NHWC
 in memory): the feature kernel writes NHWC bfloat16 directly and the correction
 kernel reads the bfloat16 NHWC residual in place, so the hand-off around the
-convolutions (cuDNN, tensor cores) needs no layout or dtype conversion.
+convolutions (cuDNN, tensor cores) needs no layout or dtype conversion.  Each
+convolution's bias and ReLU run as one in-place pass (``swe_bias_act_nhwc``)
+over its channels-last output instead of the framework's broadcast add and a
+separate activation pass; other layouts, devices and activations use torch ops.
 """
 
 from __future__ import annotations
 
+import ctypes
 from collections.abc import Sequence
 
 import torch
 import torch.nn.functional as F
 from torch import nn
 
+class _BiasAct(torch.autograd.Function):
+    """y <- act(y + bias) in place on a CUDA channels-last convolution output."""
+
+    @staticmethod
+    def forward(ctx, y, bias, relu):
+        from . import _lib
+
+        lib = _lib.load()
+        b = bias.detach().to(torch.float32).contiguous()
+        rc = lib.swe_bias_act_nhwc(ctypes.c_void_p(y.data_ptr()), y.numel(), y.shape[1], ctypes.c_void_p(b.data_ptr()),
+                                   1 if relu else 0, 1 if y.dtype == torch.bfloat16 else 0, y.device.index,
+                                   ctypes.c_void_p(torch.cuda.current_stream(y.device).cuda_stream))
+        _lib.check(rc, "swe_bias_act_nhwc")
+        ctx.mark_dirty(y)
+        ctx.relu = relu
+        ctx.save_for_backward(y)
+        return y
+
+    @staticmethod
+    def backward(ctx, g):
+        (y,) = ctx.saved_tensors
+        if ctx.relu:
+            g = g * (y > 0).to(g.dtype)
+        return g, g.float().sum(dim=(0, 2, 3)), None
+
+
+def _fusable(y: torch.Tensor) -> bool:
+    return (y.is_cuda and y.dtype in (torch.bfloat16, torch.float32) and y.dim() == 4
+            and y.is_contiguous(memory_format=torch.channels_last))
+
+
+def conv_bias_act(conv: nn.Module, x: torch.Tensor, relu: bool) -> torch.Tensor:
+    """``act(conv(x))`` with the bias and ReLU fused into one pass where the layout allows."""
+    transposed = isinstance(conv, nn.ConvTranspose2d)
+    if transposed:
+        y = F.conv_transpose2d(x, conv.weight, None, conv.stride, conv.padding)
+    else:
+        y = F.conv2d(x, conv.weight, None, conv.stride, conv.padding)
+    if conv.bias is not None and _fusable(y):
+        return _BiasAct.apply(y, conv.bias, relu)
+    if conv.bias is not None:
+        y = y + conv.bias.view(1, -1, 1, 1)
+    return F.relu(y) if relu else y
+
+
 _ACTIVATIONS = {
-    "relu": lambda: nn.ReLU(inplace=True),  # in place: each convolution's output is not needed again
+    "relu": lambda: nn.ReLU(),
     "gelu": lambda: nn.GELU(approximate="tanh"),  # Flax's default GELU is the tanh form
     "silu": lambda: nn.SiLU(),
     "tanh": lambda: nn.Tanh(),
@@ -47,8 +96,11 @@ class ConvPair(nn.Module):
         self.activation_1 = make_activation(activation)
         self.conv_2 = nn.Conv2d(cout, cout, k, padding=k // 2)
         self.activation_2 = make_activation(activation)
+        self.relu = activation.lower() == "relu"
 
     def forward(self, x: torch.Tensor) -> torch.Tensor:
+        if self.relu:
+            return conv_bias_act(self.conv_2, conv_bias_act(self.conv_1, x, True), True)
         return self.activation_2(self.conv_2(self.activation_1(self.conv_1(x))))
 
 
@@ -99,13 +151,13 @@ class ResidualUNet(nn.Module):
             x = enc(x)
             skips.append(x)
             if level + 1 < self.depth:
-                x = self.downsample[level](pad_same_stride2(x))
+                x = conv_bias_act(self.downsample[level], pad_same_stride2(x), False)
         for up, dec, skip in zip(self.upsample, self.decoders, reversed(skips[:-1])):
-            x = up(x)
+            x = conv_bias_act(up, x, False)
             if x.shape[-2:] != skip.shape[-2:]:
                 x = F.interpolate(x, size=skip.shape[-2:], mode="bilinear", align_corners=False)
             x = dec(torch.cat((x, skip), dim=1))
-        return self.residual_head(x)
+        return conv_bias_act(self.residual_head, x, False)
 
 
 def count_parameters(model: nn.Module) -> int:

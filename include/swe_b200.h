@@ -217,6 +217,14 @@ int swe_output_fields(swe_domain_t d, const float *h, const float *hu, const flo
                       float *depth, float *x_velocity, float *y_velocity, float *speed, int64_t out_pitch,
                       void *stream);
 
+/* In place y = act(y + bias[channel]) over a channels-last tensor of n elements
+ * with `channels` innermost (the bias and ReLU of a convolution of the residual
+ * U-Net, benchmark/pytorch_residual_net.py:47-76, fused into one pass).  y:
+ * device bfloat16 (bf16 = 1) or float32; bias: device float32[channels];
+ * relu = 1 applies max(., 0).  device: the CUDA device y lives on. */
+int swe_bias_act_nhwc(void *y, int64_t n, int32_t channels, const float *bias, int32_t relu, int32_t bf16,
+                      int32_t device, void *stream);
+
 /* Volume-preserving residual correction (apply_residual_correction,
  * hybrid/coupled_forecast.py:82-120), with the clip of :199-200 fused in:
  * res = clip(residual, -clip_limits, clip_limits) per channel (host

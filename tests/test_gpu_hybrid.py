@@ -276,3 +276,21 @@ def test_ensemble_advance_to_and_coupled_ensemble_match_single_domains(cuda_devi
         assert one.physics_steps_used == steps[m]
         for q in range(3):
             assert rel_l2(traj[m][q].cpu().numpy(), one.states[q].cpu().numpy()) < 1e-5
+
+
+def test_overlapped_corrector_gives_the_same_rollout(cuda_device):
+    """The corrector on a side stream (overlapping the physics) changes nothing."""
+    from hybrid_flood_b200.hybrid import run_coupled_forecast
+
+    torch.backends.cudnn.benchmark = False
+    solver, params, w, mask, state = _case(seed=12)
+    hi = _inputs(w, np.random.default_rng(6))
+    net = _small_net(6, 3, seed=4).to(cuda_device)
+    times = np.array([0.0, 30.0, 60.0])
+    a = run_coupled_forecast(solver, _dev(state, cuda_device), net, hi, times, max_substeps_per_interval=400,
+                             overlap=True)
+    b = run_coupled_forecast(solver, _dev(state, cuda_device), net, hi, times, max_substeps_per_interval=400,
+                             overlap=False)
+    assert a.physics_steps_used == b.physics_steps_used
+    for x, y in zip(a.states, b.states):
+        assert torch.equal(x, y)
