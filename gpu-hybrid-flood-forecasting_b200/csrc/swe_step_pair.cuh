@@ -46,6 +46,7 @@ struct WarpSmem {
     float left[3][kWarp];      // hi side of the strip's left x-face, per batch row
     float right[7][kWarp];     // the cell right of the strip, per batch row
     float2 ring[kRing][5][kWarp];  // [slot][field][lane]
+    double led[5][kWarp];      // float64 ledger sums per lane (vol, rain, clip, mask, outflow)
 };
 
 __device__ __forceinline__ void cp_async_8z(void* dst, const void* src, int src_bytes) {
@@ -152,13 +153,19 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
     zero_ledger();
     float maxinv = 0.f;
     // Float ledger partials cover at most one 32-row batch (64 cells per term), then go to float64.
+    // The float64 sums live in the warp's shared memory during the march, so
+    // that they hold no registers; they return to `acc` at the end.
+    if constexpr (RUN) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) sm.led[q][lane] = 0.0;
+    }
     auto flush_ledger = [&]() {
         if constexpr (RUN) {
-            acc.vol += (double)lg.vol.x + (double)lg.vol.y;
-            acc.rain += (double)lg.rain.x + (double)lg.rain.y;
-            acc.clip += (double)lg.clip.x + (double)lg.clip.y;
-            acc.mask += (double)lg.mask.x + (double)lg.mask.y;
-            acc.outflow += dtd * ((double)(lg.out_x.x + lg.out_x.y) * d.dy + (double)(lg.out_y.x + lg.out_y.y) * d.dx);
+            sm.led[0][lane] += (double)lg.vol.x + (double)lg.vol.y;
+            sm.led[1][lane] += (double)lg.rain.x + (double)lg.rain.y;
+            sm.led[2][lane] += (double)lg.clip.x + (double)lg.clip.y;
+            sm.led[3][lane] += (double)lg.mask.x + (double)lg.mask.y;
+            sm.led[4][lane] += dtd * ((double)(lg.out_x.x + lg.out_x.y) * d.dy + (double)(lg.out_y.x + lg.out_y.y) * d.dx);
             zero_ledger();
         }
     };
@@ -381,6 +388,11 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
     }
     flush_ledger();
     if constexpr (RUN) {
+        acc.vol += sm.led[0][lane];
+        acc.rain += sm.led[1][lane];
+        acc.clip += sm.led[2][lane];
+        acc.mask += sm.led[3][lane];
+        acc.outflow += sm.led[4][lane];
         acc.maxinv = nan_max(acc.maxinv, maxinv);
         // Without a mask every in-grid cell of every row received dt*rate.
         if (!MASKED && d.mult == nullptr) acc.rain_cells += (unsigned)((valid.x ? 1 : 0) + (valid.y ? 1 : 0)) * (unsigned)(r1 - r0);
