@@ -6,6 +6,8 @@
 // the device (swe::Control); the host enqueues step kernels in chunks and only
 // polls a pinned copy of the control block to learn when the run is done.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <algorithm>
 #include <cmath>
@@ -167,7 +169,7 @@ void dispatch(int V, int arith, bool run, bool masked, F&& f) {
 Plan make_plan(const swe_domain* d, int V, bool run) {
     Plan p;
     p.V = V;
-    const int rows = d->dd.rows, cols = d->dd.cols;
+    const int rows = d->dd.upd_hi - d->dd.upd_lo, cols = d->dd.cols;  // the rows the step updates
     p.nstrips = (cols + kWarp * V - 1) / (kWarp * V);
     // The occupancy query costs more than a small step: ask once per kernel instance.
     int& occ = const_cast<swe_domain*>(d)->occ_cache[V - 1][run ? 1 : 0];
@@ -264,7 +266,7 @@ int copy_plane(float* dst, int64_t dpitch, const float* src, int64_t spitch, int
 // ensemble.
 int begin_run(swe_domain* d, StateView init, const float* times_host, int n_times, double t_start,
               int n_out, int max_steps, float* out_h, float* out_hu, float* out_hv, cudaStream_t st,
-              const double* times64_host = nullptr, double* dt_log = nullptr) {
+              const double* times64_host = nullptr, double* dt_log = nullptr, int defer_plan = 0) {
     const int rows = d->dd.rows, cols = d->dd.cols;
     int rc = ensure_ping(d);
     if (rc) return rc;
@@ -306,6 +308,7 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
     c0.times64 = times64_host ? d->times64_dev : nullptr;
     c0.done_counter = d->done_counter;
     c0.dt_log = dt_log;
+    c0.defer_plan = defer_plan;
     c0.out_h = out_h;
     c0.out_hu = out_hu;
     c0.out_hv = out_hv;
@@ -897,6 +900,8 @@ int swe_domain_create(const swe_domain_desc* desc, swe_domain_t* out) {
     dd.rain_r = d->rain + q.n_rain;
     dd.n_rain = q.n_rain;
     dd.rain_scale = 1.0;
+    dd.upd_lo = 0;
+    dd.upd_hi = q.rows;
     *out = d;
     return SWE_OK;
 }
@@ -1642,6 +1647,304 @@ int swe_last_step_time(swe_domain_t d, double* ms, int64_t* step_launches) {
     SWE_CK(cudaEventElapsedTime(&f, d->time_ev[0], d->time_ev[1]));
     *ms = (double)f;
     *step_launches = d->timed_steps;
+    return SWE_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Row strips of one domain (domain decomposition across GPUs)
+// ---------------------------------------------------------------------------
+// A strip owns global rows [row_begin, row_end) and also holds the row below
+// and the row above it when they exist (halo rows, read as ordinary neighbours
+// and never updated).  One step of the whole domain is, per strip: the step
+// kernel over the owned rows (its fold keeps the strip's CFL maximum), the
+// maximum over strips (NCCL all-reduce, or a kernel when all strips are in one
+// process), plan_kernel (the next dt from that maximum, the same on every
+// strip), and the halo exchange of the new state (each strip's first and last
+// owned rows to its neighbours).
+
+}  // extern "C"
+
+namespace {
+
+// NCCL, opened at run time so that single-GPU users need no NCCL library.
+struct NcclApi {
+    ncclResult_t (*GetUniqueId)(ncclUniqueId*);
+    ncclResult_t (*CommInitRank)(ncclComm_t*, int, ncclUniqueId, int);
+    ncclResult_t (*CommDestroy)(ncclComm_t);
+    ncclResult_t (*AllReduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t, cudaStream_t);
+    ncclResult_t (*Send)(const void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
+    ncclResult_t (*Recv)(void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
+    ncclResult_t (*GroupStart)();
+    ncclResult_t (*GroupEnd)();
+    const char* (*GetErrorString)(ncclResult_t);
+};
+
+const NcclApi* nccl_api() {
+    static NcclApi api;
+    static bool ok = false;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+        if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+        if (!h) return;
+        auto sym = [&](const char* name) { return dlsym(h, name); };
+        api.GetUniqueId = reinterpret_cast<decltype(api.GetUniqueId)>(sym("ncclGetUniqueId"));
+        api.CommInitRank = reinterpret_cast<decltype(api.CommInitRank)>(sym("ncclCommInitRank"));
+        api.CommDestroy = reinterpret_cast<decltype(api.CommDestroy)>(sym("ncclCommDestroy"));
+        api.AllReduce = reinterpret_cast<decltype(api.AllReduce)>(sym("ncclAllReduce"));
+        api.Send = reinterpret_cast<decltype(api.Send)>(sym("ncclSend"));
+        api.Recv = reinterpret_cast<decltype(api.Recv)>(sym("ncclRecv"));
+        api.GroupStart = reinterpret_cast<decltype(api.GroupStart)>(sym("ncclGroupStart"));
+        api.GroupEnd = reinterpret_cast<decltype(api.GroupEnd)>(sym("ncclGroupEnd"));
+        api.GetErrorString = reinterpret_cast<decltype(api.GetErrorString)>(sym("ncclGetErrorString"));
+        ok = api.GetUniqueId && api.CommInitRank && api.CommDestroy && api.AllReduce && api.Send && api.Recv &&
+             api.GroupStart && api.GroupEnd && api.GetErrorString;
+    });
+    return ok ? &api : nullptr;
+}
+
+#define SWE_NCCL(call)                                                                             \
+    do {                                                                                           \
+        const ncclResult_t r_ = (call);                                                            \
+        if (r_ != ncclSuccess) return fail(SWE_ERR_CUDA, std::string("NCCL: ") + api->GetErrorString(r_)); \
+    } while (0)
+
+// Maximum of the strips' CFL maxima into every strip's control block (one block).
+__global__ void strips_max_kernel(Control* const* ctls, int n) {
+    __shared__ float m;
+    if (threadIdx.x == 0) {
+        float v = 0.f;
+        for (int i = 0; i < n; ++i) v = fmaxf(v, ctls[i]->maxinv);  // NaN already mapped to +inf
+        m = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) ctls[i]->maxinv = m;
+}
+
+int strip_begin(swe_domain* d, float* h, float* hu, float* hv, int64_t pitch, double t0, int n_steps,
+                cudaStream_t st) {
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    rc = ensure_ping(d);
+    if (rc) return rc;
+    // One partial per CTA of the step kernel as well as of the reduction.
+    rc = ensure_parts(d, std::max(make_plan(d, d->run_vec, true).blocks, reduce_blocks(d)));
+    if (rc) return rc;
+    const float times[2] = {(float)t0, INFINITY};
+    return begin_run(d, StateView{h, hu, hv, pitch}, times, 2, t0, 2, n_steps, nullptr, nullptr, nullptr, st,
+                     nullptr, nullptr, 1);
+}
+
+void strip_step(swe_domain* d, int k, cudaStream_t st) {
+    const Plan pl = make_plan(d, d->run_vec, true);
+    StepLaunch sl{};
+    sl.d = d->dd;
+    const int src = k & 1;
+    sl.in = StateView{d->ping[src][0], d->ping[src][1], d->ping[src][2], d->ppitch};
+    sl.out = StateOut{d->ping[src ^ 1][0], d->ping[src ^ 1][1], d->ping[src ^ 1][2], d->ppitch};
+    sl.ctl = d->ctl;
+    sl.parts = d->parts;
+    sl.nstrips = pl.nstrips;
+    sl.rows_per_warp = pl.rows_per_warp;
+    launch_step(d, pl, sl, true, st);
+}
+
+int strip_finish(swe_domain* d, float* h, float* hu, float* hv, int64_t pitch, int n_steps, swe_run_result* r,
+                 cudaStream_t st) {
+    const int fb = n_steps & 1;
+    float* outs[3] = {h, hu, hv};
+    for (int f = 0; f < 3; ++f) {
+        const int rc = copy_plane(outs[f], pitch, d->ping[fb][f], d->ppitch, d->dd.rows, d->dd.cols, st);
+        if (rc) return rc;
+    }
+    SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+    SWE_CK(cudaStreamSynchronize(st));
+    const Control& c = d->ctl_host[0];
+    r->final_time_s = c.t;
+    r->outputs_written = c.idx;
+    r->steps_used = c.steps;
+    r->status = c.status;
+    r->reserved = 0;
+    for (int i = 0; i < 6; ++i) r->ledger[i] = c.ledger[i];
+    return SWE_OK;
+}
+
+}  // namespace
+
+struct swe_comm {
+    ncclComm_t comm = nullptr;
+    int world = 1, rank = 0, device = 0;
+};
+
+extern "C" {
+
+int swe_comm_unique_id(void* id_out) {
+    if (!id_out) return fail(SWE_ERR_INVALID, "null argument");
+    const NcclApi* api = nccl_api();
+    if (!api) return fail(SWE_ERR_INVALID, "NCCL (libnccl.so.2) could not be loaded");
+    ncclUniqueId id;
+    SWE_NCCL(api->GetUniqueId(&id));
+    std::memcpy(id_out, &id, sizeof(id));
+    return SWE_OK;
+}
+
+int swe_comm_create(const void* id, int32_t world, int32_t rank, swe_comm_t* out) {
+    if (!id || !out || world < 1 || rank < 0 || rank >= world) return fail(SWE_ERR_INVALID, "bad communicator arguments");
+    *out = nullptr;
+    const NcclApi* api = nccl_api();
+    if (!api) return fail(SWE_ERR_INVALID, "NCCL (libnccl.so.2) could not be loaded");
+    ncclUniqueId uid;
+    std::memcpy(&uid, id, sizeof(uid));
+    auto* c = new swe_comm();
+    c->world = world;
+    c->rank = rank;
+    cudaGetDevice(&c->device);
+    const ncclResult_t r = api->CommInitRank(&c->comm, world, uid, rank);
+    if (r != ncclSuccess) {
+        delete c;
+        return fail(SWE_ERR_CUDA, std::string("NCCL: ") + api->GetErrorString(r));
+    }
+    *out = c;
+    return SWE_OK;
+}
+
+int swe_comm_destroy(swe_comm_t c) {
+    if (!c) return SWE_OK;
+    const NcclApi* api = nccl_api();
+    if (api && c->comm) api->CommDestroy(c->comm);
+    delete c;
+    return SWE_OK;
+}
+
+int swe_strip_create(const swe_domain_desc* global, int32_t row_begin, int32_t row_end, swe_domain_t* out) {
+    if (!global || !out) return fail(SWE_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (row_begin < 0 || row_end <= row_begin || row_end > global->rows)
+        return fail(SWE_ERR_INVALID, "need 0 <= row_begin < row_end <= rows");
+    const int lo = row_begin > 0 ? row_begin - 1 : 0;
+    const int hi = row_end < global->rows ? row_end + 1 : row_end;
+    swe_domain_desc q = *global;
+    const int64_t off = (int64_t)lo * global->cols;
+    q.rows = hi - lo;
+    q.bed = global->bed + off;
+    q.manning_n = global->manning_n + off;
+    q.domain_mask = global->domain_mask + off;
+    q.rainfall_multiplier = global->rainfall_multiplier ? global->rainfall_multiplier + off : nullptr;
+    swe_domain_t d = nullptr;
+    const int rc = swe_domain_create(&q, &d);
+    if (rc) return rc;
+    d->dd.upd_lo = row_begin - lo;
+    d->dd.upd_hi = row_end - lo;
+    *out = d;
+    return SWE_OK;
+}
+
+int swe_strip_layout(swe_domain_t d, int32_t* local_rows, int32_t* upd_lo, int32_t* upd_hi) {
+    if (!d || !local_rows || !upd_lo || !upd_hi) return fail(SWE_ERR_INVALID, "null argument");
+    *local_rows = d->dd.rows;
+    *upd_lo = d->dd.upd_lo;
+    *upd_hi = d->dd.upd_hi;
+    return SWE_OK;
+}
+
+int swe_strips_advance(const swe_domain_t* strips, int32_t n, float* const* h, float* const* hu, float* const* hv,
+                       const int64_t* pitch, int32_t n_steps, double t0, swe_run_result* results, void* stream) {
+    if (!strips || n < 1 || !h || !hu || !hv || !pitch || !results || n_steps < 0)
+        return fail(SWE_ERR_INVALID, "bad strip arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (int i = 0; i < n; ++i) {
+        if (!strips[i] || strips[i]->dd.cols != strips[0]->dd.cols) return fail(SWE_ERR_INVALID, "strips must share cols");
+        if (i + 1 < n && (strips[i]->dd.upd_hi != strips[i]->dd.rows - 1 || strips[i + 1]->dd.upd_lo != 1))
+            return fail(SWE_ERR_INVALID, "strips must be given bottom to top, each with its neighbours' halo rows");
+    }
+    for (int i = 0; i < n; ++i) {
+        const int rc = strip_begin(strips[i], h[i], hu[i], hv[i], pitch[i], t0, n_steps, st);
+        if (rc) return rc;
+    }
+    Control** ctls = nullptr;
+    SWE_CK(cudaMalloc(&ctls, sizeof(Control*) * (size_t)n));
+    std::vector<Control*> hc(n);
+    for (int i = 0; i < n; ++i) hc[i] = strips[i]->ctl;
+    int rc = SWE_OK;
+    auto plan_all = [&]() {
+        strips_max_kernel<<<1, 32, 0, st>>>(ctls, n);
+        for (int i = 0; i < n; ++i) plan_kernel<<<1, 1, 0, st>>>(strips[i]->dd, strips[i]->ctl);
+    };
+    if (cudaMemcpyAsync(ctls, hc.data(), sizeof(Control*) * (size_t)n, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        rc = fail(SWE_ERR_CUDA, "copy of the strip table failed");
+    if (!rc) plan_all();
+    const int cols = strips[0]->dd.cols;
+    for (int k = 0; k < n_steps && !rc; ++k) {
+        for (int i = 0; i < n; ++i) strip_step(strips[i], k, st);
+        plan_all();
+        const int b = (k + 1) & 1;
+        for (int i = 0; i + 1 < n && !rc; ++i) {
+            swe_domain* L = strips[i];
+            swe_domain* U = strips[i + 1];
+            for (int f = 0; f < 3 && !rc; ++f) {
+                const float* lo_row = L->ping[b][f] + (int64_t)(L->dd.upd_hi - 1) * L->ppitch;
+                const float* up_row = U->ping[b][f] + (int64_t)U->dd.upd_lo * U->ppitch;
+                if (cudaMemcpyAsync(U->ping[b][f], lo_row, sizeof(float) * cols, cudaMemcpyDeviceToDevice, st) ||
+                    cudaMemcpyAsync(L->ping[b][f] + (int64_t)(L->dd.rows - 1) * L->ppitch, up_row, sizeof(float) * cols,
+                                    cudaMemcpyDeviceToDevice, st))
+                    rc = fail(SWE_ERR_CUDA, "halo copy failed");
+            }
+        }
+    }
+    if (!rc && cudaGetLastError() != cudaSuccess) rc = fail(SWE_ERR_CUDA, "strip step launch failed");
+    for (int i = 0; i < n && !rc; ++i) rc = strip_finish(strips[i], h[i], hu[i], hv[i], pitch[i], n_steps, &results[i], st);
+    cudaStreamSynchronize(st);
+    cudaFree(ctls);
+    if (rc) return rc;
+    for (int i = 0; i < n; ++i)
+        if (results[i].status) return fail(results[i].status, "a strip stopped with an error status");
+    return SWE_OK;
+}
+
+int swe_strip_advance_nccl(swe_domain_t d, swe_comm_t comm, int32_t rank_below, int32_t rank_above, float* h,
+                           float* hu, float* hv, int64_t pitch, int32_t n_steps, double t0, swe_run_result* result,
+                           void* stream) {
+    if (!d || !comm || !result || n_steps < 0) return fail(SWE_ERR_INVALID, "bad strip arguments");
+    const NcclApi* api = nccl_api();
+    if (!api) return fail(SWE_ERR_INVALID, "NCCL (libnccl.so.2) could not be loaded");
+    if ((rank_below >= 0) != (d->dd.upd_lo == 1) || (rank_above >= 0) != (d->dd.upd_hi == d->dd.rows - 1))
+        return fail(SWE_ERR_INVALID, "neighbour ranks must match the strip's halo rows");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = strip_begin(d, h, hu, hv, pitch, t0, n_steps, st);
+    if (rc) return rc;
+    const int cols = d->dd.cols;
+    auto plan = [&]() -> int {
+        SWE_NCCL(api->AllReduce(&d->ctl->maxinv, &d->ctl->maxinv, 1, ncclFloat, ncclMax, comm->comm, st));
+        plan_kernel<<<1, 1, 0, st>>>(d->dd, d->ctl);
+        return SWE_OK;
+    };
+    rc = plan();
+    for (int k = 0; k < n_steps && !rc; ++k) {
+        strip_step(d, k, st);
+        rc = plan();
+        if (rc) break;
+        const int b = (k + 1) & 1;
+        SWE_NCCL(api->GroupStart());
+        for (int f = 0; f < 3; ++f) {
+            float* plane = d->ping[b][f];
+            if (rank_below >= 0) {
+                SWE_NCCL(api->Send(plane + (int64_t)d->dd.upd_lo * d->ppitch, cols, ncclFloat, rank_below, comm->comm, st));
+                SWE_NCCL(api->Recv(plane, cols, ncclFloat, rank_below, comm->comm, st));
+            }
+            if (rank_above >= 0) {
+                SWE_NCCL(api->Send(plane + (int64_t)(d->dd.upd_hi - 1) * d->ppitch, cols, ncclFloat, rank_above,
+                                   comm->comm, st));
+                SWE_NCCL(api->Recv(plane + (int64_t)(d->dd.rows - 1) * d->ppitch, cols, ncclFloat, rank_above,
+                                   comm->comm, st));
+            }
+        }
+        SWE_NCCL(api->GroupEnd());
+    }
+    if (!rc && cudaGetLastError() != cudaSuccess) rc = fail(SWE_ERR_CUDA, "strip step launch failed");
+    if (!rc) rc = strip_finish(d, h, hu, hv, pitch, n_steps, result, st);
+    if (rc) return rc;
+    if (result->status) return fail(result->status, "the strip stopped with an error status");
     return SWE_OK;
 }
 

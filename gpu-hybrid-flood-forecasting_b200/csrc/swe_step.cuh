@@ -59,6 +59,10 @@ struct DomainDev {
     const double* rain_r;  // rates (m/s)
     int n_rain;
     double rain_scale;     // multiplies every rate (1 = the hyetograph as given)
+    // Rows the step updates and the reductions cover: [upd_lo, upd_hi).  A row
+    // strip of a decomposed domain also holds its neighbours' boundary rows
+    // (halo rows) outside that range: read as ordinary neighbours, never updated.
+    int upd_lo, upd_hi;
 };
 
 struct StateView {
@@ -99,11 +103,11 @@ struct Control {
     float* out_hv;
     int64_t out_plane;            // rows * cols
     double ledger[6];             // volume0, volume, rain_in, outflow, clip_gain, mask_loss
+    int defer_plan;               // 1: the fold leaves maxinv (NaN as +inf) for plan_kernel to use
 };
 
 struct Partial {
     float maxinv;
-    int bad;
     double vol, rain, outflow, clip, mask;
 };
 
@@ -381,9 +385,16 @@ struct StepAccum {
 // Reduce per-thread accumulators over the CTA in a fixed order, write the CTA
 // partial, and let the last CTA to finish fold all partials (again in a fixed
 // order, so the ledger is bitwise reproducible) and advance the control block.
+// Bookkeeping once the next step is planned: its dt in the log, the ensemble's
+// completion counter.
+__device__ __forceinline__ void after_plan(Control& c) {
+    if (!c.done && c.dt_log) c.dt_log[c.steps] = c.dt;  // steps < max_steps while not done
+    if (c.done && c.done_counter) atomicAdd(c.done_counter, 1u);
+}
+
 template <int THREADS>
 __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts, Accum acc,
-                                bool init, bool failed = false, int part = -1, int nparts = -1) {
+                                bool init, int part = -1, int nparts = -1) {
     // One partial per CTA of this domain: by default the launch's CTAs; the
     // ensemble kernel passes the CTA's slot within its member instead.
     if (part < 0) {
@@ -394,10 +405,6 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     __shared__ float s_max[W];
     __shared__ double s_sum[5][W];
     __shared__ bool s_last;
-    __shared__ int s_bad;
-    if (threadIdx.x == 0) s_bad = 0;
-    __syncthreads();
-    if (failed) s_bad = 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     acc.maxinv = warp_max(acc.maxinv);
     acc.vol = warp_sum(acc.vol);
@@ -417,7 +424,6 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     if (threadIdx.x == 0) {
         Partial p;
         p.maxinv = s_max[0];
-        p.bad = s_bad;
         p.vol = s_sum[0][0]; p.rain = s_sum[1][0]; p.outflow = s_sum[2][0];
         p.clip = s_sum[3][0]; p.mask = s_sum[4][0];
         for (int w = 1; w < W; ++w) {
@@ -436,16 +442,13 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     // Fixed-order fold of all CTA partials: thread t folds partials t, t+T, ...
     Accum a;
     a.zero();
-    int bad = 0;
     const volatile Partial* vp = parts;
     for (int b = threadIdx.x; b < nparts; b += THREADS) {
-        bad |= vp[b].bad;
         a.maxinv = nan_max(a.maxinv, vp[b].maxinv);
         a.vol += vp[b].vol; a.rain += vp[b].rain; a.outflow += vp[b].outflow;
         a.clip += vp[b].clip; a.mask += vp[b].mask;
     }
     __syncthreads();
-    bad = __syncthreads_or(bad);
     a.maxinv = warp_max(a.maxinv);
     a.vol = warp_sum(a.vol); a.rain = warp_sum(a.rain); a.outflow = warp_sum(a.outflow);
     a.clip = warp_sum(a.clip); a.mask = warp_sum(a.mask);
@@ -487,17 +490,26 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     }
     c.maxinv = mx;
     c.counter = 0;
-    plan_next(d, c);
-    if (bad) {  // a bounded device wait ran out: stop the run and report it
-        c.status = 6;  // SWE_ERR_TIMEOUT
-        c.done = 1;
-        c.snap = -1;
-        c.reach = -1;
+    if (c.defer_plan) {
+        // A row strip: the CFL maximum of the whole domain is formed across the
+        // strips first (NaN kept as +inf so that a maximum carries it), then
+        // plan_kernel plans the step.
+        if (!(mx == mx)) c.maxinv = INFINITY;
+    } else {
+        plan_next(d, c);
+        after_plan(c);
     }
-    if (!c.done && c.dt_log) c.dt_log[c.steps] = c.dt;  // steps < max_steps while not done
-    if (c.done && c.done_counter) atomicAdd(c.done_counter, 1u);
     *ctl = c;
     __threadfence();
+}
+
+// Plans the next step of a row strip from the domain-wide CFL maximum now in
+// ctl->maxinv (single thread).
+__global__ void plan_kernel(const DomainDev d, Control* ctl) {
+    Control c = *ctl;
+    plan_next(d, c);
+    after_plan(c);
+    *ctl = c;
 }
 
 // ---------------------------------------------------------------------------
@@ -550,14 +562,14 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
     const int gw = blockIdx.x * NW + wib;
     const int strip = gw % p.nstrips;
     const int chunk = gw / p.nstrips;
-    const int r0 = chunk * p.rows_per_warp;
-    const int r1 = min(r0 + p.rows_per_warp, d.rows);
+    const int r0 = d.upd_lo + chunk * p.rows_per_warp;
+    const int r1 = min(r0 + p.rows_per_warp, d.upd_hi);
     const int x0w = strip * kWarp * V;
     const int c0 = x0w + lane * V;
     StepAccum acc;
     acc.zero();
 
-    if (r0 < d.rows) {
+    if (r0 < d.upd_hi) {
         Cell A[V], B[V], C[V];
         float yT0[V], yT1[V], yT2[V];
         // Bottom face of the chunk: rows r0-1 (A) and r0 (B).
@@ -790,10 +802,10 @@ __global__ void __launch_bounds__(THREADS) reduce_kernel(const DomainDev d, cons
     const Consts& k = d.k;
     Accum acc;
     acc.zero();
-    const int64_t n = (int64_t)d.rows * d.cols;
+    const int64_t n = (int64_t)(d.upd_hi - d.upd_lo) * d.cols;
     for (int64_t i = (int64_t)blockIdx.x * THREADS + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * THREADS) {
-        const int r = (int)(i / d.cols), c = (int)(i - (int64_t)r * d.cols);
+        const int r = d.upd_lo + (int)(i / d.cols), c = (int)(i - (int64_t)(r - d.upd_lo) * d.cols);
         const float h = s.h[(int64_t)r * s.pitch + c];
         const float hu = s.hu[(int64_t)r * s.pitch + c];
         const float hv = s.hv[(int64_t)r * s.pitch + c];

@@ -419,11 +419,11 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
     const int gw = blockIdx.x * NW + wib;
     const int strip = gw % p.nstrips;
     const int chunk = gw / p.nstrips;
-    const int r0 = chunk * p.rows_per_warp;
-    const int r1 = min(r0 + p.rows_per_warp, d.rows);
+    const int r0 = d.upd_lo + chunk * p.rows_per_warp;
+    const int r1 = min(r0 + p.rows_per_warp, d.upd_hi);
     StepAccum acc;
     acc.zero();
-    if (r0 < d.rows)
+    if (r0 < d.upd_hi)
         march_pair<M, RUN, MASKED>(d, p.in, p.out, s, snap, dtd, p.ctl, r0, r1, strip * kWarp * 2,
                                   s_warp[wib], acc);
     if constexpr (RUN) {
@@ -502,7 +502,7 @@ ensemble_step_kernel(const MemberDev* __restrict__ members, const int2* __restri
         a.outflow = acc.outflow;
         a.clip = acc.clip;
         a.mask = acc.mask;
-        finish_run_step<THREADS>(md.d, md.ctl, md.parts, a, false, false, item.y, md.ncta);
+        finish_run_step<THREADS>(md.d, md.ctl, md.parts, a, false, item.y, md.ncta);
     }
 }
 

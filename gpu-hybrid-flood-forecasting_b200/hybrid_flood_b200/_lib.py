@@ -22,6 +22,7 @@ SWE_ARITH_EXACT = 0
 SWE_ARITH_FAST = 1
 
 SWE_NOALLOC_MAX_CELLS = 16_777_216
+SWE_COMM_ID_BYTES = 128
 
 #: Every entry point ``include/swe_b200.h`` declares.
 EXPORTS = (
@@ -57,6 +58,13 @@ EXPORTS = (
     "swe_ensemble_set_timing",
     "swe_ensemble_last_step_time",
     "swe_ensemble_last_launch_count",
+    "swe_strip_create",
+    "swe_strip_layout",
+    "swe_strips_advance",
+    "swe_comm_unique_id",
+    "swe_comm_create",
+    "swe_comm_destroy",
+    "swe_strip_advance_nccl",
     "swe_last_error",
     "swe_version",
 )
@@ -160,6 +168,15 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_ensemble_set_timing": (ctypes.c_int, [_vp, _i32]),
         "swe_ensemble_last_step_time": (ctypes.c_int, [_vp, ctypes.POINTER(_f64), ctypes.POINTER(_i64)]),
         "swe_ensemble_last_launch_count": (ctypes.c_int64, [_vp]),
+        "swe_strip_create": (ctypes.c_int, [ctypes.POINTER(DomainDesc), _i32, _i32, ctypes.POINTER(_vp)]),
+        "swe_strip_layout": (ctypes.c_int, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
+        "swe_strips_advance": (ctypes.c_int, [_vp, _i32, _vp, _vp, _vp, _vp, _i32, _f64, ctypes.POINTER(RunResult),
+                                              _vp]),
+        "swe_comm_unique_id": (ctypes.c_int, [_vp]),
+        "swe_comm_create": (ctypes.c_int, [_vp, _i32, _i32, ctypes.POINTER(_vp)]),
+        "swe_comm_destroy": (ctypes.c_int, [_vp]),
+        "swe_strip_advance_nccl": (ctypes.c_int, [_vp, _vp, _i32, _i32, _vp, _vp, _vp, _i64, _i32, _f64,
+                                                  ctypes.POINTER(RunResult), _vp]),
         "swe_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
         "swe_version": (ctypes.c_char_p, []),
     }

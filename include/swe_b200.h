@@ -278,6 +278,45 @@ int swe_ensemble_set_timing(swe_ensemble_t e, int32_t enable);
 int swe_ensemble_last_step_time(swe_ensemble_t e, double *ms, int64_t *steps);
 int64_t swe_ensemble_last_launch_count(swe_ensemble_t e);
 
+/* ---- Row strips: one domain split across GPUs ----------------------------
+ * (No counterpart in the reference, which runs one domain on one device; the
+ * strip step is the reference step, finite_volume_step, over the strip's rows.)
+ * A strip owns global rows [row_begin, row_end) and also holds the row below
+ * and the row above when they exist (halo rows: read as neighbours, never
+ * updated), so its local planes have row_end - row_begin + (number of halo
+ * rows) rows, local row 0 being global row max(row_begin - 1, 0).  Every step
+ * of the whole domain: the step kernel over the owned rows, the CFL maximum
+ * over all strips, the same dt planned on every strip, and the exchange of the
+ * new boundary rows.  The result matches one domain stepped whole, bit for bit. */
+typedef struct swe_comm *swe_comm_t;
+#define SWE_COMM_ID_BYTES 128
+
+/* Create a strip of the domain `global` describes (its fields on the host or the
+ * device, as for swe_domain_create). */
+int swe_strip_create(const swe_domain_desc *global, int32_t row_begin, int32_t row_end, swe_domain_t *out);
+/* The strip's local row count and its owned local rows [upd_lo, upd_hi). */
+int swe_strip_layout(swe_domain_t d, int32_t *local_rows, int32_t *upd_lo, int32_t *upd_hi);
+
+/* n strips of one domain, bottom to top, all on the current device (one
+ * process): n_steps steps from t0; (h, hu, hv)[i] are strip i's local planes,
+ * updated in place (halo rows included).  The maximum over strips is a kernel and
+ * the exchange device-to-device copies. */
+int swe_strips_advance(const swe_domain_t *strips, int32_t n, float *const *h, float *const *hu,
+                       float *const *hv, const int64_t *pitch, int32_t n_steps, double t0,
+                       swe_run_result *results, void *stream);
+
+/* One strip per process and GPU over NCCL (opened at run time, libnccl.so.2):
+ * the maximum is an all-reduce and the exchange point-to-point sends between
+ * neighbour ranks (-1 where the strip has no halo row on that side).  Every rank
+ * must call it with the same n_steps and t0.  swe_comm_unique_id writes
+ * SWE_COMM_ID_BYTES bytes on one rank; pass them to swe_comm_create on all. */
+int swe_comm_unique_id(void *id_out);
+int swe_comm_create(const void *id, int32_t world, int32_t rank, swe_comm_t *out);
+int swe_comm_destroy(swe_comm_t c);
+int swe_strip_advance_nccl(swe_domain_t d, swe_comm_t comm, int32_t rank_below, int32_t rank_above, float *h,
+                           float *hu, float *hv, int64_t pitch, int32_t n_steps, double t0,
+                           swe_run_result *result, void *stream);
+
 /* Largest cell count swe_max_inverse_dt_noalloc accepts (a 4096 x 4096 grid). */
 #define SWE_NOALLOC_MAX_CELLS 16777216
 
