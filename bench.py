@@ -81,6 +81,8 @@ def _args():
     ap.add_argument("--no-training", action="store_true")
     ap.add_argument("--training-members", type=int, default=16)
     ap.add_argument("--training-size", type=int, default=1024)
+    ap.add_argument("--decompose", action="store_true",
+                    help="also time the single domain split into row strips, one per GPU over NCCL (strong scaling)")
     return ap.parse_args()
 
 
@@ -417,6 +419,36 @@ def _training(args, dev):
             "peak_mem_gb": torch.cuda.max_memory_allocated(dev) / 1e9}
 
 
+def _decomposed(args, dev, rank: int, world: int):
+    """The same 2048x2048 domain split into one row strip per rank (halo rows,
+    domain-wide dt, NCCL exchange): all ranks' cell-updates over the slowest rank's
+    time (strong scaling of a fixed domain)."""
+    import torch
+
+    from hybrid_flood_b200.decomposition import NcclStrip
+    from hybrid_flood_b200.sharding import max_over_ranks
+    from hybrid_flood_b200.workloads import as_member
+
+    w, depth = _workload(args.rows, args.cols)
+    strip = NcclStrip(as_member(w), rank=rank, world=world, arithmetic=args.arith, device=dev)
+    z = np.zeros_like(depth)
+    local = strip.local_state([torch.tensor(a, device=dev) for a in (depth, z, z)])
+    t, _, _ = strip.advance_(local, args.spinup + args.warmup, 0.0)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    strip.advance_(local, args.steps, t)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    return {"value": w.bed.size * args.steps / (ms / 1e3), "unit": "cell-updates/s", "scaling": "strong",
+            "strips": world, "ms_per_step": ms / args.steps,
+            "workload": f"urban {args.rows}x{args.cols} split into {world} row strips (NCCL halo exchange)"}
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
@@ -518,6 +550,7 @@ def run_b200(args, rank: int, world: int):
                "call": "B200ShallowWaterSolver.run(host NumPy state, [0, window]) + final state to host",
                "steps_per_call": steps_e2e / reps, "wall_s": wall}
 
+    dec = _decomposed(args, dev, rank, world) if args.decompose else None
     ens = None
     if not args.no_ensemble:
         ens = _ensemble(args, dev, rank, world)
@@ -566,6 +599,8 @@ def run_b200(args, rank: int, world: int):
         line["adjoint"] = adj
     if hyb:
         line["hybrid"] = hyb
+    if dec:
+        line["decomposed"] = dec
     if trn:
         line["training"] = trn
     if not args.no_cpu_baseline:
