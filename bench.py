@@ -12,22 +12,26 @@ for 200 steps before warm-up, so the timed steps see moving water.
 
 A "step" is one finite-volume time step over the whole grid: CFL dt from the
 previous state's reduction, fluxes, update, friction, masks, and the next CFL
-reduction plus FP64 ledger, all inside the fused kernel.  ``value`` is
-cell-updates/s over K timed steps (CUDA events on the launching stream; the
-per-step working set is 134 MB -- five input planes and three output planes of
-16.8 MB -- above the 126 MB L2, so no flush is inserted).  ``e2e`` times
-``B200ShallowWaterSolver.run`` called with HOST NumPy state: host->device copy of
-the state, the adaptive run over the same simulated window, and the
-device->host copy of the final state.
+reduction plus FP64 ledger, all inside the fused kernel.  The state is loaded
+into the solver's resident buffers before timing; the timed region is exactly
+K step launches (whole 32-step CUDA graphs where K allows), bracketed by a
+barrier and a device synchronisation, timed with CUDA events on the launching
+stream.  ``value`` is cell-updates/s over those K steps.  The per-step working
+set is 134 MB (five input planes and three output planes of 16.8 MB), above the
+126 MB L2, so no flush is inserted.  ``e2e`` times ``B200ShallowWaterSolver.run``
+called with HOST (pinned NumPy-backed) state over a forecast window with six
+output times, the host->device copy of the state and the device->host copy of
+every recorded snapshot inside the timed region.
 
 Multi-GPU: one process per GPU, each advancing its own replica of the domain
-(the single domain does not shard without a halo exchange, which this step
-does not implement); ``value`` is the sum over ranks divided by the slowest
-rank's time ("replicas", weak scaling).
+(weak scaling, no collective in the timed region); ``value`` is the sum over
+ranks divided by the slowest rank's time.  ``--decompose`` also times the one
+domain split into row strips across the ranks (halo exchange over NCCL, strong
+scaling) in a sub-object.
 
 ``--impl reference`` times the CPU implementation of the same path: the C
 restatement of the reference step (oracle/swe_oracle.c, OpenMP over all host
-threads) on the same workload, a few whole-grid steps per timed step.
+threads) on the same workload and the same config, whole-grid steps.
 """
 
 from __future__ import annotations
@@ -37,7 +41,6 @@ import json
 import os
 import pathlib
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -52,9 +55,9 @@ METRIC = "cell-updates/s (plain single-domain step, 2048x2048 urban)"
 BYTES_PER_CELL = 32  # h, hu, hv, bed, n^2 read (20 B) + h, hu, hv written (12 B)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fast-arithmetic
 # step_kernel_pair launch on the default 2048x2048 workload, per cell-update, from an
-# ncu --set full capture of that launch (103.8 MB read + 12.8 MB written): reported as
-# roofline.traffic for that configuration only.
+# ncu capture of that launch: reported as roofline.traffic for that configuration only.
 NCU_TRAFFIC_PER_CELL = (103.774976e6 + 12.771328e6) / 4194304
+REFERENCE_MAX_STEPS = 200  # whole-grid steps the CPU reference arm times at most
 
 
 def _args():
@@ -68,7 +71,9 @@ def _args():
     ap.add_argument("--cols", type=int, default=2048)
     ap.add_argument("--spinup", type=int, default=200)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=500, help="steps of the e2e forecast window")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-members", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=200)
@@ -87,13 +92,17 @@ def _args():
 
 
 def _workload(rows, cols):
-    from hybrid_flood_b200.workloads import urban
+    from hybrid_flood_b200.workloads import street_depth, urban
 
     w = urban(rows, cols)
-    plane = 0.003 * (cols * 1.0 - (np.arange(cols) + 0.5))[None, :]
-    streets = (w.bed - plane) < 1.0
-    depth = np.where(streets, 0.05, 0.0).astype(np.float32)
-    return w, depth
+    return w, street_depth(w)
+
+
+def _config(args, world: int) -> dict:
+    """The workload description both arms print (the driver compares them)."""
+    return {"workload": f"urban {args.rows}x{args.cols} dx=1m (plain forward at scale)",
+            "cells_per_gpu": args.rows * args.cols, "parallelism": f"replicas{world}",
+            "l2": "per-step working set 134 MB > 126 MB L2; no flush", "spinup_steps": args.spinup}
 
 
 def _peaks():
@@ -105,69 +114,93 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi SM clock / throttle-reason sampler running during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML in a
+    background thread every ~0.5 ms; :meth:`summary` keeps the samples taken
+    between :meth:`mark_start` and :meth:`mark_end` (the timed region)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.lines: list[str] = []
+    def __init__(self, device):
+        self.device = device
+        self.samples: list[tuple[float, float, int]] = []
+        self.window = (None, None)
+        self.max_mhz = None
+        self._stop = threading.Event()
         self._t = None
+        self._nv = None
+        self._h = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+            import torch
+
+            nv.nvmlInit()
+            self._nv = nv
+            props = torch.cuda.get_device_properties(self.device)
+            try:
+                bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+                self._h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:  # noqa: BLE001 - fall back to the ordinal
+                self._h = nv.nvmlDeviceGetHandleByIndex(self.device.index or 0)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self._h, nv.NVML_CLOCK_SM))
+            self._t = threading.Thread(target=self._run, daemon=True)
             self._t.start()
-            deadline = time.time() + 3.0
-            while not self.lines and time.time() < deadline:  # sampler running before timing
-                time.sleep(0.02)
-            self.lines.clear()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+        except Exception:  # noqa: BLE001 - no NVML: report no samples
+            self._nv = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self._h))
+                self.samples.append((time.perf_counter(), mhz, rs))
+            except Exception:  # noqa: BLE001
+                return
+            time.sleep(0.0005)
+
+    def mark_start(self):
+        self.window = (time.perf_counter(), None)
+
+    def mark_end(self):
+        self.window = (self.window[0], time.perf_counter())
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=2)
+        if self._nv is not None:
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            if self._t:
-                self._t.join(timeout=2)
+                self._nv.nvmlShutdown()
+            except Exception:  # noqa: BLE001
+                pass
 
     def summary(self) -> dict:
-        mhz, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                mhz.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[5:9]):
-                if flag.lower().startswith("active"):
+        t0, t1 = self.window
+        inside = [s for s in self.samples if t0 is not None and t1 is not None and t0 <= s[0] <= t1]
+        reasons = set()
+        nv = self._nv
+        for _, _, rs in inside:
+            for name, attr in self.REASONS:
+                bit = getattr(nv, attr, 0) if nv is not None else 0
+                if bit and rs & bit:
                     reasons.add(name)
-        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(mhz)}
+        return {"sm_mhz": statistics.median([s[1] for s in inside]) if inside else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(reasons), "samples": len(inside),
+                "source": "NVML, every ~0.5 ms during the timed region"}
 
 
 def _cpu_port_time(w, depth, steps: int, threads: int):
-    """Time the C restatement of the reference step on the host: (s/step, cells)."""
+    """Time the C restatement of the reference step on the host: (s/step, cells).
+
+    Each step is the reference loop's CFL reduction plus the step
+    (``numpy_solver/shallow_water_2d.py:402-412``)."""
     from oracle import cport
     from oracle import swe_numpy as O
 
@@ -188,9 +221,89 @@ def _cpu_port_time(w, depth, steps: int, threads: int):
     return el / steps, w.bed.size
 
 
+def _numpy_reference_time(w, depth, steps: int) -> dict:
+    """The reference NumPy solver's loop (restated bit for bit in
+    ``oracle/swe_numpy.py``, pinned to the reference's own outputs): NumPy's
+    elementwise operations use one core."""
+    from oracle import swe_numpy as O
+
+    p = O.make_params(w.bed, w.manning_n, w.domain_mask, **w.solver_kwargs())
+    st = O.initial_state(p, depth_m=depth)
+    t = 0.0
+    st = O.finite_volume_step(st, p, O.compute_cfl_dt(st, p), t)  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = O.compute_cfl_dt(st, p)
+        st = O.finite_volume_step(st, p, dt, t)
+        t += dt
+    el = time.perf_counter() - t0
+    return {"value": w.bed.size * steps / el, "unit": "cell-updates/s", "cores": 1, "steps": steps,
+            "s_per_step": el / steps, "grid": list(w.shape)}
+
+
+def _cpu_legs(w, depth) -> dict:
+    """Host-core baselines of the same path: the C port on every host thread,
+    the reference NumPy loop on one core (the 256x256 and 2048x2048 cases), and
+    JAX-CPU when JAX is importable."""
+    from hybrid_flood_b200.workloads import tilted_bumps
+    from oracle import cport
+
+    threads = cport.default_threads()
+    per_step, cells = _cpu_port_time(w, depth, 3, threads)
+    out = {"value": cells / per_step, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+           "sample": "3 whole-grid steps of the same workload (C restatement, every host thread)",
+           "host_cores": os.cpu_count()}
+    small = tilted_bumps(256, 256)
+    out["numpy"] = {"config0_256x256": _numpy_reference_time(small, np.full(small.shape, 0.01, np.float32), 20),
+                    "config1_2048x2048": _numpy_reference_time(w, depth, 3),
+                    "kind": "reference NumPy loop (oracle/swe_numpy.py, bit-identical to the reference)"}
+    try:
+        import jax  # noqa: F401
+
+        out["jax_cpu"] = "importable but not timed by this bench"
+    except ImportError:
+        out["jax_cpu"] = "unavailable on this box (jax is not installed)"
+    return out
+
+
+def _parity(args, w, depth, dev) -> dict:
+    """100 CFL steps of the measured workload on the GPU against the float32 and
+    float64 C restatements (relative L2 of the depth)."""
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver
+    from oracle import cport
+    from oracle import swe_numpy as O
+
+    n = 100
+    s = B200ShallowWaterSolver(w.bed, w.manning_n, w.domain_mask, **w.solver_kwargs(), arithmetic=args.arith,
+                               device=dev)
+    init = O.initial_state(O.make_params(w.bed, w.manning_n, w.domain_mask, **w.solver_kwargs()), depth_m=depth)
+    got, t_gpu, _, _ = s.advance(list(init), n, 0.0)
+    h = got.h.cpu().numpy().astype(np.float64)
+    out = {"steps": n, "simulated_s": t_gpu}
+    for name, dtype in (("f32", np.float32), ("f64", np.float64)):
+        p = O.make_params(w.bed, w.manning_n, w.domain_mask, dtype=dtype, **w.solver_kwargs())
+        d = cport.Domain(p)
+        st, t = O.State(*(np.asarray(a, dtype) for a in init)), 0.0
+        for _ in range(n):
+            dt = d.cfl_dt(st)
+            st = d.step(st, dt, t)
+            t += dt
+        ref = np.asarray(st.h, np.float64)
+        out[f"rel_l2_vs_{name}"] = float(np.linalg.norm(h - ref) / np.linalg.norm(ref))
+        if name == "f64":
+            out["f32_oracle_vs_f64"] = float(np.linalg.norm(np.asarray(f32_h, np.float64) - ref) / np.linalg.norm(ref))
+        else:
+            f32_h = st.h
+    out["bar"] = "rel L2 depth <= 1e-5 after 100 steps (vs the float32 restatement)"
+    return out
+
+
 def _ensemble(args, dev, rank: int, world: int):
     """Batched 64-member ensemble vs the same members run one by one (plain path).
 
+    Both are timed the same way: the members' states are loaded first, and the
+    CUDA events bracket only the step launches (the ensemble's 50-step graphs;
+    the plain solvers' resident steps, member after member, on one stream).
     With N ranks the members are partitioned across GPUs (cell-balanced bin
     pack, no per-step collective): the value is all members' cell-updates over
     the slowest rank's time (strong scaling of a fixed ensemble)."""
@@ -211,9 +324,9 @@ def _ensemble(args, dev, rank: int, world: int):
     states = ens.initial_states(depths)
     ens.advance_(states, 50)  # spin-up
     tune_states = [type(s)(*(t.clone() for t in s)) for s in states]
-    best = ens.autotune(tune_states, candidates=(8, 16, 32, 64), steps=10, cache=None)
+    best = ens.autotune(tune_states, candidates=(16, 32, 64, 128), steps=50, cache=None)
     del tune_states
-    ens.advance_(states, 10)  # warm-up (graph capture)
+    ens.advance_(states, 50)  # warm-up (graph capture)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
@@ -224,21 +337,21 @@ def _ensemble(args, dev, rank: int, world: int):
     cells = sum(cells_all)
     value = cells * n / (ms / 1e3)
     worst_ledger = max_over_ranks(max(ledger_error(r[2]) for r in res))
-    # Plain path, member after member, same steps (each member its own solver).
+    # Plain path, member after member, same steps (each member its own solver, resident state).
     solvers = [B200ShallowWaterSolver(m["bed"], m["manning_n"], m["domain_mask"],
                                       **{k: v for k, v in m.items() if k not in ("bed", "manning_n", "domain_mask")},
                                       arithmetic=args.arith, device=dev) for m in members]
-    plain_states = [s.initial_state(depth_m=d) for s, d in zip(solvers, depths)]
-    for s, st in zip(solvers, plain_states):
-        s.advance_(st, 10)
+    for s, d in zip(solvers, depths):
+        s.resident_load(s.initial_state(depth_m=d))
+        s.resident_steps(100)  # spin-up and warm-up (graph capture)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for s, st in zip(solvers, plain_states):
-        s.advance_(st, args.ensemble_steps)
+    for s in solvers:
+        s.resident_steps(args.ensemble_steps)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     plain_ms = max_over_ranks(e0.elapsed_time(e1))
@@ -250,6 +363,7 @@ def _ensemble(args, dev, rank: int, world: int):
         "steps": n, "ms_per_step": ms / n, "rows_per_warp": best,
         "roofline_frac": BYTES_PER_CELL * value / world / 1e9 / peak, "peak_kind": kind,
         "plain_sequential_value": plain_value, "speedup_vs_plain_sequential": value / plain_value,
+        "timing": "both arms: CUDA events around the step launches only (states loaded beforehand)",
         "ledger_rel_error_max": worst_ledger, "gpu_launches": ens.last_launch_count(),
         "workload": f"{len(ws_all)} urban members from {{256^2, 512^2, 1024^2, 768x1536}}, dx=1m, "
                     "rain x LogNormal(0.4), n x U(0.8,1.2), seeds 1000+m",
@@ -450,29 +564,78 @@ def _decomposed(args, dev, rank: int, world: int):
 
 
 def run_reference(args, rank: int, world: int):
+    """The CPU implementation of the same path on the host cores: the C
+    restatement of the reference step on every host thread, whole-grid steps of
+    the same workload (``min(K, 200)`` timed, after ``min(W, 3)`` warm-up)."""
     if rank != 0:
         return
     from oracle import cport
 
     w, depth = _workload(args.rows, args.cols)
     threads = cport.default_threads()
-    per_step, cells = _cpu_port_time(w, depth, max(1, args.steps // 40) + 1, threads)
-    # "steps" of this arm: K whole-grid steps, each timed as measured above.
-    k = args.steps
+    k = max(1, min(args.steps, REFERENCE_MAX_STEPS))
+    per_step, cells = _cpu_port_time(w, depth, k, threads)
     value = cells / per_step
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
-        "n_gpus": args.gpus, "steps": k, "warmup": args.warmup,
+        "n_gpus": args.gpus, "steps": k, "steps_requested": args.steps, "warmup": args.warmup,
         "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"urban {args.rows}x{args.cols} dx=1m (plain forward at scale)",
-                   "cells": cells, "arith": "C restatement, IEEE float32, no FMA"},
+        "config": _config(args, world),
+        "arith": "C restatement, IEEE float32, no FMA",
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"{max(1, args.steps // 40) + 1} whole-grid steps of the same workload"},
+                         "sample": f"{k} whole-grid steps of the same workload"},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def _e2e(args, solver, state, t_sim, dev, world: int) -> dict:
+    """``B200ShallowWaterSolver.run`` with host state: a forecast window of about
+    ``--e2e-steps`` steps with six output times; the state goes in from pinned
+    host memory and every recorded snapshot comes back to pinned host memory
+    inside the timed region."""
+    import torch
+
+    cells = solver.shape[0] * solver.shape[1]
+    host = [t.cpu().numpy().copy() for t in state]
+    pinned = [torch.from_numpy(a).pin_memory() for a in host]
+    # The simulated window that --e2e-steps steps cover from this state.
+    probe = type(state)(*(t.clone() for t in state))
+    t_end, _, _ = solver.advance_(probe, args.e2e_steps, 0.0)
+    del probe
+    window = float(np.float32(t_end))
+    times = np.linspace(0.0, window, 6).astype(np.float32)
+    n_out = len(times)
+    outs_host = [torch.empty((n_out, *solver.shape), dtype=torch.float32).pin_memory() for _ in range(3)]
+    stream = torch.cuda.current_stream(dev)
+
+    def once():
+        r = solver.run(pinned, times)
+        for dst, src in zip(outs_host, r.states):
+            dst.copy_(src, non_blocking=True)
+        return r
+
+    once()  # warm-up of the run path (graphs, plans)
+    torch.cuda.synchronize(dev)
+    reps = 3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record(stream)
+    steps = 0
+    for _ in range(reps):
+        steps += once().steps_used
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - w0
+    ms = e0.elapsed_time(e1)
+    plane = cells * 4
+    return {"value": cells * steps * world / (ms / 1e3), "unit": "cell-updates/s",
+            "h2d_bytes_per_step": int(3 * plane * reps / max(steps, 1)),
+            "d2h_bytes_per_step": int(3 * plane * n_out * reps / max(steps, 1)),
+            "call": "B200ShallowWaterSolver.run(pinned host state, 6 output times) + every snapshot to pinned host",
+            "steps_per_call": steps / reps, "simulated_window_s": window, "wall_s": wall}
 
 
 def run_b200(args, rank: int, world: int):
@@ -483,10 +646,12 @@ def run_b200(args, rank: int, world: int):
     dev = torch.device("cuda", local)
     dist = None
     if world > 1:
+        import datetime
+
         import torch.distributed as dist_mod
 
         dist = dist_mod
-        dist.init_process_group("nccl", device_id=dev)
+        dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(seconds=300))
     from hybrid_flood_b200.solver import B200ShallowWaterSolver, ledger_error
 
     w, depth = _workload(args.rows, args.cols)
@@ -494,62 +659,36 @@ def run_b200(args, rank: int, world: int):
                                     arithmetic=args.arith, device=dev)
     state = solver.initial_state(depth_m=depth)
     t_sim, _, _ = solver.advance_(state, args.spinup, 0.0)
-    t_sim, _, _ = solver.advance_(state, args.warmup, t_sim)
     cells = w.bed.size
     stream = torch.cuda.current_stream(dev)
-    solver.set_timing(True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
+    # Resident state: W untimed warm-up steps, then exactly K timed steps.
+    solver.resident_load(state, t_sim)
+    solver.resident_steps(args.warmup)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t_before = t_sim
-    with ClockSampler(local) as clocks:
+    with ClockSampler(dev) as clocks:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        clocks.mark_start()
         start.record(stream)
-        t_sim, steps_used, ledger = solver.advance_(state, args.steps, t_sim)
+        solver.resident_steps(args.steps)
         end.record(stream)
         torch.cuda.synchronize(dev)
+        clocks.mark_end()
     if dist:
         dist.barrier()
     ms = start.elapsed_time(end)
-    kernel_ms, kernel_launches = solver.last_step_time()
     launches = solver.last_launch_count()
+    t_before = t_sim
+    t_sim, steps_done, ledger = solver.resident_store(state)
     if dist:
-        tt = torch.tensor([ms, kernel_ms], device=dev, dtype=torch.float64)
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms, kernel_ms = float(tt[0]), float(tt[1])
+        ms = float(tt[0])
     value = cells * args.steps * world / (ms / 1e3)
     window = t_sim - t_before
 
-    # End to end through the public API with host buffers.
-    e2e = None
-    if not args.no_e2e:
-        host = [t.cpu().numpy().copy() for t in state]
-        pinned = [torch.from_numpy(a).pin_memory() for a in host]
-        times = np.asarray([0.0, window], np.float32)
-        r = solver.run(pinned, times)  # warm-up of the run path
-        torch.cuda.synchronize(dev)
-        reps = 3
-        t0 = time.perf_counter()
-        e_start = torch.cuda.Event(enable_timing=True)
-        e_end = torch.cuda.Event(enable_timing=True)
-        e_start.record(stream)
-        steps_e2e = 0
-        for _ in range(reps):
-            r = solver.run(pinned, times)
-            out = r.states.h[-1].cpu(), r.states.hu[-1].cpu(), r.states.hv[-1].cpu()
-            steps_e2e += r.steps_used
-        e_end.record(stream)
-        torch.cuda.synchronize(dev)
-        e_ms = e_start.elapsed_time(e_end)
-        wall = time.perf_counter() - t0
-        del out
-        plane = cells * 4
-        e2e = {"value": cells * steps_e2e * world / (e_ms / 1e3), "unit": "cell-updates/s",
-               "h2d_bytes_per_step": int(3 * plane * reps / max(steps_e2e, 1)),
-               "d2h_bytes_per_step": int(3 * plane * reps / max(steps_e2e, 1)),
-               "call": "B200ShallowWaterSolver.run(host NumPy state, [0, window]) + final state to host",
-               "steps_per_call": steps_e2e / reps, "wall_s": wall}
-
+    e2e = None if args.no_e2e else _e2e(args, solver, state, t_sim, dev, world)
     dec = _decomposed(args, dev, rank, world) if args.decompose else None
     ens = None
     if not args.no_ensemble:
@@ -563,36 +702,39 @@ def run_b200(args, rank: int, world: int):
     trn = None
     if not args.no_training and rank == 0:
         trn = _training(args, dev)
+    par = None
+    if not args.no_parity and rank == 0:
+        par = _parity(args, w, depth, dev)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
     peak, peak_kind = _peaks()
-    per_launch_ms = kernel_ms / max(kernel_launches, 1)
+    per_launch_ms = ms / args.steps
     achieved = BYTES_PER_CELL * cells / (per_launch_ms / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": f"urban {args.rows}x{args.cols} dx=1m (plain forward at scale)",
-                   "cells_per_gpu": cells, "arith": args.arith, "parallelism": f"replicas{world}",
-                   "l2": "per-step working set 134 MB > 126 MB L2; no flush",
-                   "simulated_window_s": window, "spinup_steps": args.spinup},
+        "data": "synthetic", "config": _config(args, world), "arith": args.arith,
+        "simulated_window_s": window,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": (NCU_TRAFFIC_PER_CELL * cells
                                  if (args.rows, args.cols, args.arith) == (2048, 2048, "fast") else None),
                      "traffic_unit": "bytes per launch (ncu capture of the same launch)",
-                     "kernel": "step_kernel (fused step + CFL + ledger)",
+                     "kernel": "step_kernel_pair (fused step + CFL + ledger), the only kernel of the timed region",
                      "bytes_per_cell": BYTES_PER_CELL, "peak_kind": peak_kind,
-                     "kernel_ms_per_launch": per_launch_ms},
+                     "kernel_ms_per_launch": per_launch_ms,
+                     "duration": "timed-region CUDA events / K (back-to-back step launches, gaps included)"},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "ledger_rel_error": ledger_error(ledger),
     }
     if e2e:
         line["e2e"] = e2e
+    if par:
+        line["parity"] = par
     if ens:
         line["ensemble"] = ens
     if adj:
@@ -604,13 +746,7 @@ def run_b200(args, rank: int, world: int):
     if trn:
         line["training"] = trn
     if not args.no_cpu_baseline:
-        from oracle import cport
-
-        threads = cport.default_threads()
-        per_step, _ = _cpu_port_time(w, depth, 3, threads)
-        line["cpu_baseline"] = {"value": cells / per_step, "unit": "cell-updates/s",
-                                "cores": threads, "kind": "port",
-                                "sample": "3 whole-grid steps of the same workload (C restatement)"}
+        line["cpu_baseline"] = _cpu_legs(w, depth)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -7,6 +7,8 @@
 // polls a pinned copy of the control block to learn when the run is done.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
+#include <time.h>
+#include <unistd.h>
 #include <nccl.h>
 
 #include <algorithm>
@@ -118,6 +120,18 @@ struct swe_domain {
     double* corr_sums = nullptr;    // volume sums of the residual correction
     float* corr_prov = nullptr;     // provisional-depth plane of the correction
     unsigned* done_counter = nullptr;  // set by an ensemble: shared completion counter
+    // CUDA graph of kChunk run-mode steps starting from ping buffer 0, and the
+    // inputs it was captured with (a change of any of them re-captures it).
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t chunk_graph = nullptr;
+    const Partial* chunk_graph_parts = nullptr;
+    double chunk_graph_rain_scale = 0.0;
+    int chunk_graph_rows = 0;
+    // Resident run (swe_resident_*): state kept in the ping buffers between calls.
+    bool resident = false;
+    int64_t resident_steps = 0;  // steps enqueued since swe_resident_load (buffer parity)
+    // Row strip of a decomposed domain: its owned global rows and the domain's rows.
+    int strip_row_begin = -1, strip_row_end = -1, strip_total_rows = -1;
 };
 
 namespace {
@@ -268,6 +282,7 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
               int n_out, int max_steps, float* out_h, float* out_hu, float* out_hv, cudaStream_t st,
               const double* times64_host = nullptr, double* dt_log = nullptr, int defer_plan = 0) {
     const int rows = d->dd.rows, cols = d->dd.cols;
+    d->resident = false;  // any run replaces a resident state
     int rc = ensure_ping(d);
     if (rc) return rc;
     rc = ensure_parts(d, reduce_blocks(d));
@@ -323,6 +338,78 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
     return SWE_OK;
 }
 
+// Steps per poll of the run driver and per captured step graph (even, so that
+// a graph always starts and ends on ping buffer 0).
+constexpr int kChunk = 32;
+
+// Run-mode launch of step k of a run (buffer parity k & 1).
+StepLaunch run_launch(const swe_domain* d, const Plan& pl, int64_t k) {
+    StepLaunch sl{};
+    sl.d = d->dd;
+    sl.ctl = d->ctl;
+    sl.parts = d->parts;
+    sl.nstrips = pl.nstrips;
+    sl.rows_per_warp = pl.rows_per_warp;
+    const int src = (int)(k & 1);
+    sl.in = StateView{d->ping[src][0], d->ping[src][1], d->ping[src][2], d->ppitch};
+    sl.out = StateOut{d->ping[src ^ 1][0], d->ping[src ^ 1][1], d->ping[src ^ 1][2], d->ppitch};
+    return sl;
+}
+
+// The kChunk-step graph from ping buffer 0, captured on a private stream (the
+// caller's stream may be the legacy default stream, which cannot be captured).
+// Its kernel parameters hold the domain record by value, so a change of the
+// partials buffer, the rain scale or the plan re-captures it.
+int chunk_graph(swe_domain* d, const Plan& pl, cudaGraphExec_t* out) {
+    if (d->chunk_graph && d->chunk_graph_parts == d->parts && d->chunk_graph_rain_scale == d->dd.rain_scale &&
+        d->chunk_graph_rows == pl.rows_per_warp) {
+        *out = d->chunk_graph;
+        return SWE_OK;
+    }
+    if (d->chunk_graph) {
+        cudaGraphExecDestroy(d->chunk_graph);
+        d->chunk_graph = nullptr;
+    }
+    if (!d->cap_stream) SWE_CK(cudaStreamCreateWithFlags(&d->cap_stream, cudaStreamNonBlocking));
+    SWE_CK(cudaStreamBeginCapture(d->cap_stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kChunk; ++k) launch_step(d, pl, run_launch(d, pl, k), true, d->cap_stream);
+    cudaGraph_t g = nullptr;
+    SWE_CK(cudaStreamEndCapture(d->cap_stream, &g));
+    const cudaError_t err = cudaGraphInstantiate(&d->chunk_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (err != cudaSuccess) {
+        d->chunk_graph = nullptr;
+        return fail(SWE_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(err));
+    }
+    d->chunk_graph_parts = d->parts;
+    d->chunk_graph_rain_scale = d->dd.rain_scale;
+    d->chunk_graph_rows = pl.rows_per_warp;
+    *out = d->chunk_graph;
+    return SWE_OK;
+}
+
+// Enqueue steps k0 .. k0+n-1 of the current run: whole kChunk-step graphs where
+// the step index is even and a whole chunk remains, single launches elsewhere.
+int enqueue_run_steps(swe_domain* d, int64_t k0, int64_t n, cudaStream_t st) {
+    const Plan pl = make_plan(d, d->run_vec, true);
+    int64_t k = k0;
+    const int64_t end = k0 + n;
+    while (k < end) {
+        if ((k & 1) == 0 && end - k >= kChunk) {
+            cudaGraphExec_t g = nullptr;
+            const int rc = chunk_graph(d, pl, &g);
+            if (rc) return rc;
+            SWE_CK(cudaGraphLaunch(g, st));
+            k += kChunk;
+        } else {
+            launch_step(d, pl, run_launch(d, pl, k), true, st);
+            ++k;
+        }
+    }
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
 // Shared run driver for swe_run and swe_advance.
 int run_driver(swe_domain* d, StateView init, const float* times_host, int n_times,
                double t_start, int n_out, int max_steps, float* out_h, float* out_hu,
@@ -340,24 +427,13 @@ int run_driver(swe_domain* d, StateView init, const float* times_host, int n_tim
     d->launches = 1;
     d->timed_valid = false;
     if (d->timing) SWE_CK(cudaEventRecord(d->time_ev[0], st));
-    StepLaunch sl{};
-    sl.d = d->dd;
-    sl.ctl = d->ctl;
-    sl.parts = d->parts;
-    sl.nstrips = pl.nstrips;
-    sl.rows_per_warp = pl.rows_per_warp;
-    const int K = 32;
+    const int K = kChunk;
     int chunk = 0;
     bool finished = false;
     while (!finished) {
         const int64_t todo = std::min<int64_t>(K, (int64_t)max_steps - launched);
-        for (int64_t k = 0; k < todo; ++k) {
-            const int src = (int)((launched + k) & 1);
-            sl.in = StateView{d->ping[src][0], d->ping[src][1], d->ping[src][2], d->ppitch};
-            sl.out = StateOut{d->ping[src ^ 1][0], d->ping[src ^ 1][1], d->ping[src ^ 1][2], d->ppitch};
-            launch_step(d, pl, sl, true, st);
-        }
-        SWE_CK(cudaGetLastError());
+        rc = enqueue_run_steps(d, launched, todo, st);
+        if (rc) return rc;
         launched += todo;
         d->launches += todo;
         const int slot = chunk & 1;
@@ -411,6 +487,8 @@ void free_domain(swe_domain* d) {
         if (d->poll_ev[i]) cudaEventDestroy(d->poll_ev[i]);
         if (d->time_ev[i]) cudaEventDestroy(d->time_ev[i]);
     }
+    if (d->chunk_graph) cudaGraphExecDestroy(d->chunk_graph);
+    if (d->cap_stream) cudaStreamDestroy(d->cap_stream);
     delete d;
 }
 
@@ -1139,6 +1217,65 @@ int swe_advance(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, i
 
 int64_t swe_last_launch_count(swe_domain_t d) { return d ? d->launches : -1; }
 
+int swe_resident_load(swe_domain_t d, const float* h, const float* hu, const float* hv, int64_t pitch,
+                      double start_s, void* stream) {
+    if (!d) return fail(SWE_ERR_INVALID, "null domain");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    if (!std::isfinite(start_s)) return fail(SWE_ERR_INVALID, "start time must be finite");
+    rc = ensure_ping(d);
+    if (rc) return rc;
+    rc = ensure_parts(d, std::max(make_plan(d, d->run_vec, true).blocks, reduce_blocks(d)));
+    if (rc) return rc;
+    // An open-ended run: no output target within reach and no step cap, so the
+    // control block stops the steps only on a non-finite CFL maximum.
+    const float times[2] = {(float)start_s, INFINITY};
+    rc = begin_run(d, StateView{h, hu, hv, pitch}, times, 2, start_s, 2, INT32_MAX, nullptr, nullptr, nullptr,
+                   static_cast<cudaStream_t>(stream));
+    if (rc) return rc;
+    d->resident = true;
+    d->resident_steps = 0;
+    d->launches = 1;
+    return SWE_OK;
+}
+
+int swe_resident_steps(swe_domain_t d, int32_t n_steps, void* stream) {
+    if (!d) return fail(SWE_ERR_INVALID, "null domain");
+    if (!d->resident) return fail(SWE_ERR_INVALID, "no resident state: call swe_resident_load first");
+    if (n_steps < 0) return fail(SWE_ERR_INVALID, "n_steps must be >= 0");
+    const int rc = enqueue_run_steps(d, d->resident_steps, n_steps, static_cast<cudaStream_t>(stream));
+    if (rc) return rc;
+    d->resident_steps += n_steps;
+    d->launches = n_steps;
+    return SWE_OK;
+}
+
+int swe_resident_store(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, swe_run_result* result,
+                       void* stream) {
+    if (!d || !result) return fail(SWE_ERR_INVALID, "null argument");
+    if (!d->resident) return fail(SWE_ERR_INVALID, "no resident state: call swe_resident_load first");
+    int rc = check_state_ptrs(h, hu, hv, pitch, d->dd.cols);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int fb = (int)(d->resident_steps & 1);
+    float* outs[3] = {h, hu, hv};
+    for (int f = 0; f < 3; ++f) {
+        rc = copy_plane(outs[f], pitch, d->ping[fb][f], d->ppitch, d->dd.rows, d->dd.cols, st);
+        if (rc) return rc;
+    }
+    SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+    SWE_CK(cudaStreamSynchronize(st));
+    const Control& c = d->ctl_host[0];
+    result->final_time_s = c.t;
+    result->outputs_written = 0;
+    result->steps_used = c.steps;
+    result->status = c.status;
+    result->reserved = 0;
+    for (int i = 0; i < 6; ++i) result->ledger[i] = c.ledger[i];
+    if (c.status == SWE_ERR_NONFINITE) return fail(SWE_ERR_NONFINITE, "non-finite values reached the CFL reduction");
+    return SWE_OK;
+}
+
 int swe_advance_to(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, double t_start,
                    double t_target, int32_t max_steps, double* dt_log, swe_run_result* result, void* stream) {
     if (!d || !result) return fail(SWE_ERR_INVALID, "null argument");
@@ -1670,8 +1807,10 @@ namespace {
 // NCCL, opened at run time so that single-GPU users need no NCCL library.
 struct NcclApi {
     ncclResult_t (*GetUniqueId)(ncclUniqueId*);
-    ncclResult_t (*CommInitRank)(ncclComm_t*, int, ncclUniqueId, int);
+    ncclResult_t (*CommInitRankConfig)(ncclComm_t*, int, ncclUniqueId, int, ncclConfig_t*);
     ncclResult_t (*CommDestroy)(ncclComm_t);
+    ncclResult_t (*CommAbort)(ncclComm_t);
+    ncclResult_t (*CommGetAsyncError)(ncclComm_t, ncclResult_t*);
     ncclResult_t (*AllReduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t, cudaStream_t);
     ncclResult_t (*Send)(const void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
     ncclResult_t (*Recv)(void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
@@ -1690,36 +1829,58 @@ const NcclApi* nccl_api() {
         if (!h) return;
         auto sym = [&](const char* name) { return dlsym(h, name); };
         api.GetUniqueId = reinterpret_cast<decltype(api.GetUniqueId)>(sym("ncclGetUniqueId"));
-        api.CommInitRank = reinterpret_cast<decltype(api.CommInitRank)>(sym("ncclCommInitRank"));
+        api.CommInitRankConfig = reinterpret_cast<decltype(api.CommInitRankConfig)>(sym("ncclCommInitRankConfig"));
         api.CommDestroy = reinterpret_cast<decltype(api.CommDestroy)>(sym("ncclCommDestroy"));
+        api.CommAbort = reinterpret_cast<decltype(api.CommAbort)>(sym("ncclCommAbort"));
+        api.CommGetAsyncError = reinterpret_cast<decltype(api.CommGetAsyncError)>(sym("ncclCommGetAsyncError"));
         api.AllReduce = reinterpret_cast<decltype(api.AllReduce)>(sym("ncclAllReduce"));
         api.Send = reinterpret_cast<decltype(api.Send)>(sym("ncclSend"));
         api.Recv = reinterpret_cast<decltype(api.Recv)>(sym("ncclRecv"));
         api.GroupStart = reinterpret_cast<decltype(api.GroupStart)>(sym("ncclGroupStart"));
         api.GroupEnd = reinterpret_cast<decltype(api.GroupEnd)>(sym("ncclGroupEnd"));
         api.GetErrorString = reinterpret_cast<decltype(api.GetErrorString)>(sym("ncclGetErrorString"));
-        ok = api.GetUniqueId && api.CommInitRank && api.CommDestroy && api.AllReduce && api.Send && api.Recv &&
-             api.GroupStart && api.GroupEnd && api.GetErrorString;
+        ok = api.GetUniqueId && api.CommInitRankConfig && api.CommDestroy && api.CommAbort &&
+             api.CommGetAsyncError && api.AllReduce && api.Send && api.Recv && api.GroupStart && api.GroupEnd &&
+             api.GetErrorString;
     });
     return ok ? &api : nullptr;
 }
 
-#define SWE_NCCL(call)                                                                             \
-    do {                                                                                           \
-        const ncclResult_t r_ = (call);                                                            \
-        if (r_ != ncclSuccess) return fail(SWE_ERR_CUDA, std::string("NCCL: ") + api->GetErrorString(r_)); \
-    } while (0)
+// Maximum of the strips' CFL maxima into every strip's control block (one
+// block).  The control blocks travel as a kernel parameter, so a step needs no
+// device table.
+constexpr int kMaxLocalStrips = 64;
+struct StripCtls {
+    Control* c[kMaxLocalStrips];
+    int n;
+};
 
-// Maximum of the strips' CFL maxima into every strip's control block (one block).
-__global__ void strips_max_kernel(Control* const* ctls, int n) {
+__global__ void strips_max_kernel(const StripCtls t) {
     __shared__ float m;
     if (threadIdx.x == 0) {
         float v = 0.f;
-        for (int i = 0; i < n; ++i) v = fmaxf(v, ctls[i]->maxinv);  // NaN already mapped to +inf
+        for (int i = 0; i < t.n; ++i) v = fmaxf(v, t.c[i]->maxinv);  // NaN already mapped to +inf
         m = v;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) ctls[i]->maxinv = m;
+    for (int i = threadIdx.x; i < t.n; i += blockDim.x) t.c[i]->maxinv = m;
+}
+
+// Local rows of a strip that take part in the halo exchange: the first and the
+// last owned row go to the neighbour below and above, and arrive in local row
+// 0 and local row rows-1 (the halo rows).  The one-process exchange and the
+// NCCL exchange both use these offsets.
+struct HaloRows {
+    int send_below, recv_below;  // valid when the strip has a halo row below (upd_lo == 1)
+    int send_above, recv_above;  // valid when the strip has a halo row above (upd_hi == rows - 1)
+};
+
+HaloRows halo_rows(const swe_domain* d) {
+    return HaloRows{d->dd.upd_lo, 0, d->dd.upd_hi - 1, d->dd.rows - 1};
+}
+
+float* plane_row(swe_domain* d, int buf, int f, int row) {
+    return d->ping[buf][f] + (int64_t)row * d->ppitch;
 }
 
 int strip_begin(swe_domain* d, float* h, float* hu, float* hv, int64_t pitch, double t0, int n_steps,
@@ -1738,16 +1899,7 @@ int strip_begin(swe_domain* d, float* h, float* hu, float* hv, int64_t pitch, do
 
 void strip_step(swe_domain* d, int k, cudaStream_t st) {
     const Plan pl = make_plan(d, d->run_vec, true);
-    StepLaunch sl{};
-    sl.d = d->dd;
-    const int src = k & 1;
-    sl.in = StateView{d->ping[src][0], d->ping[src][1], d->ping[src][2], d->ppitch};
-    sl.out = StateOut{d->ping[src ^ 1][0], d->ping[src ^ 1][1], d->ping[src ^ 1][2], d->ppitch};
-    sl.ctl = d->ctl;
-    sl.parts = d->parts;
-    sl.nstrips = pl.nstrips;
-    sl.rows_per_warp = pl.rows_per_warp;
-    launch_step(d, pl, sl, true, st);
+    launch_step(d, pl, run_launch(d, pl, k), true, st);
 }
 
 int strip_finish(swe_domain* d, float* h, float* hu, float* hv, int64_t pitch, int n_steps, swe_run_result* r,
@@ -1770,12 +1922,75 @@ int strip_finish(swe_domain* d, float* h, float* hu, float* hv, int64_t pitch, i
     return SWE_OK;
 }
 
+// Seconds the host waits for NCCL work before it aborts the communicator
+// (SWE_NCCL_TIMEOUT_S, default 120): a rank that never arrives then ends the
+// others' collectives with an error instead of leaving them waiting.
+double nccl_timeout_s() {
+    if (const char* e = std::getenv("SWE_NCCL_TIMEOUT_S")) {
+        const double v = std::atof(e);
+        if (v > 0) return v;
+    }
+    return 120.0;
+}
+
+double now_s() {
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
 }  // namespace
 
 struct swe_comm {
     ncclComm_t comm = nullptr;
     int world = 1, rank = 0, device = 0;
+    int* status_dev = nullptr;     // agreement flag (device int)
+    int* status_host = nullptr;    // pinned copy of it
+    cudaEvent_t ev = nullptr;      // completion of the enqueued NCCL work
+    bool aborted = false;
 };
+
+namespace {
+
+// Finishes a non-blocking NCCL call: waits (bounded) while the communicator
+// reports ncclInProgress.
+ncclResult_t nccl_settle(const NcclApi* api, swe_comm* c, ncclResult_t r) {
+    const double deadline = now_s() + nccl_timeout_s();
+    while (r == ncclInProgress) {
+        if (now_s() > deadline) return ncclSystemError;
+        usleep(100);
+        if (api->CommGetAsyncError(c->comm, &r) != ncclSuccess) return ncclSystemError;
+    }
+    return r;
+}
+
+int nccl_abort(const NcclApi* api, swe_comm* c, const std::string& why) {
+    if (c->comm && !c->aborted) {
+        api->CommAbort(c->comm);
+        c->aborted = true;
+        c->comm = nullptr;
+    }
+    return fail(SWE_ERR_CUDA, "NCCL: " + why + " (communicator aborted; create a new one)");
+}
+
+// Waits for the work enqueued on `st` so far, at most the NCCL timeout; aborts
+// the communicator when that runs out or NCCL reports an asynchronous error.
+int nccl_wait(const NcclApi* api, swe_comm* c, cudaStream_t st) {
+    SWE_CK(cudaEventRecord(c->ev, st));
+    const double deadline = now_s() + nccl_timeout_s();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(c->ev);
+        if (q == cudaSuccess) return SWE_OK;
+        if (q != cudaErrorNotReady) return fail(SWE_ERR_CUDA, std::string("strip step: ") + cudaGetErrorString(q));
+        ncclResult_t ae = ncclSuccess;
+        if (api->CommGetAsyncError(c->comm, &ae) == ncclSuccess && ae != ncclSuccess && ae != ncclInProgress)
+            return nccl_abort(api, c, api->GetErrorString(ae));
+        if (now_s() > deadline) return nccl_abort(api, c, "timed out waiting for the other ranks");
+        usleep(50);
+    }
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -1784,7 +1999,8 @@ int swe_comm_unique_id(void* id_out) {
     const NcclApi* api = nccl_api();
     if (!api) return fail(SWE_ERR_INVALID, "NCCL (libnccl.so.2) could not be loaded");
     ncclUniqueId id;
-    SWE_NCCL(api->GetUniqueId(&id));
+    const ncclResult_t r = api->GetUniqueId(&id);
+    if (r != ncclSuccess) return fail(SWE_ERR_CUDA, std::string("NCCL: ") + api->GetErrorString(r));
     std::memcpy(id_out, &id, sizeof(id));
     return SWE_OK;
 }
@@ -1800,10 +2016,27 @@ int swe_comm_create(const void* id, int32_t world, int32_t rank, swe_comm_t* out
     c->world = world;
     c->rank = rank;
     cudaGetDevice(&c->device);
-    const ncclResult_t r = api->CommInitRank(&c->comm, world, uid, rank);
-    if (r != ncclSuccess) {
+    auto bail = [&](int code) {
+        if (c->ev) cudaEventDestroy(c->ev);
+        cudaFree(c->status_dev);
+        if (c->status_host) cudaFreeHost(c->status_host);
         delete c;
-        return fail(SWE_ERR_CUDA, std::string("NCCL: ") + api->GetErrorString(r));
+        return code;
+    };
+    if (cudaMalloc(&c->status_dev, sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&c->status_host, sizeof(int)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(SWE_ERR_CUDA, "communicator scratch allocation failed"));
+    // Non-blocking communicator: the host bounds every wait and can abort.
+    ncclConfig_t cfg = NCCL_CONFIG_INITIALIZER;
+    cfg.blocking = 0;
+    ncclResult_t r = api->CommInitRankConfig(&c->comm, world, uid, rank, &cfg);
+    if (r == ncclInProgress && c->comm) r = nccl_settle(api, c, r);
+    if (r != ncclSuccess) {
+        if (c->comm) api->CommAbort(c->comm);
+        c->comm = nullptr;
+        return bail(fail(SWE_ERR_CUDA, std::string("NCCL: communicator creation failed or timed out: ") +
+                                           api->GetErrorString(r)));
     }
     *out = c;
     return SWE_OK;
@@ -1812,7 +2045,10 @@ int swe_comm_create(const void* id, int32_t world, int32_t rank, swe_comm_t* out
 int swe_comm_destroy(swe_comm_t c) {
     if (!c) return SWE_OK;
     const NcclApi* api = nccl_api();
-    if (api && c->comm) api->CommDestroy(c->comm);
+    if (api && c->comm && !c->aborted) api->CommDestroy(c->comm);
+    if (c->ev) cudaEventDestroy(c->ev);
+    cudaFree(c->status_dev);
+    if (c->status_host) cudaFreeHost(c->status_host);
     delete c;
     return SWE_OK;
 }
@@ -1836,6 +2072,9 @@ int swe_strip_create(const swe_domain_desc* global, int32_t row_begin, int32_t r
     if (rc) return rc;
     d->dd.upd_lo = row_begin - lo;
     d->dd.upd_hi = row_end - lo;
+    d->strip_row_begin = row_begin;
+    d->strip_row_end = row_end;
+    d->strip_total_rows = global->rows;
     *out = d;
     return SWE_OK;
 }
@@ -1852,28 +2091,36 @@ int swe_strips_advance(const swe_domain_t* strips, int32_t n, float* const* h, f
                        const int64_t* pitch, int32_t n_steps, double t0, swe_run_result* results, void* stream) {
     if (!strips || n < 1 || !h || !hu || !hv || !pitch || !results || n_steps < 0)
         return fail(SWE_ERR_INVALID, "bad strip arguments");
+    if (n > kMaxLocalStrips) return fail(SWE_ERR_INVALID, "at most 64 strips in one process");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int dev = 0;
+    SWE_CK(cudaGetDevice(&dev));
     for (int i = 0; i < n; ++i) {
-        if (!strips[i] || strips[i]->dd.cols != strips[0]->dd.cols) return fail(SWE_ERR_INVALID, "strips must share cols");
-        if (i + 1 < n && (strips[i]->dd.upd_hi != strips[i]->dd.rows - 1 || strips[i + 1]->dd.upd_lo != 1))
-            return fail(SWE_ERR_INVALID, "strips must be given bottom to top, each with its neighbours' halo rows");
+        const swe_domain* s = strips[i];
+        if (!s || s->strip_total_rows < 0) return fail(SWE_ERR_INVALID, "every entry must be a strip (swe_strip_create)");
+        if (s->device != dev) return fail(SWE_ERR_INVALID, "every strip must live on the current device");
+        if (s->dd.cols != strips[0]->dd.cols || s->strip_total_rows != strips[0]->strip_total_rows)
+            return fail(SWE_ERR_INVALID, "strips must come from one domain (same rows and cols)");
     }
+    // Adjacent slices of the same domain, bottom to top, covering all its rows.
+    if (strips[0]->strip_row_begin != 0 || strips[n - 1]->strip_row_end != strips[0]->strip_total_rows)
+        return fail(SWE_ERR_INVALID, "strips must cover the domain from its first to its last row");
+    for (int i = 0; i + 1 < n; ++i)
+        if (strips[i]->strip_row_end != strips[i + 1]->strip_row_begin)
+            return fail(SWE_ERR_INVALID, "strips must be given bottom to top, each starting where the previous ends");
     for (int i = 0; i < n; ++i) {
         const int rc = strip_begin(strips[i], h[i], hu[i], hv[i], pitch[i], t0, n_steps, st);
         if (rc) return rc;
     }
-    Control** ctls = nullptr;
-    SWE_CK(cudaMalloc(&ctls, sizeof(Control*) * (size_t)n));
-    std::vector<Control*> hc(n);
-    for (int i = 0; i < n; ++i) hc[i] = strips[i]->ctl;
-    int rc = SWE_OK;
+    StripCtls table{};
+    table.n = n;
+    for (int i = 0; i < n; ++i) table.c[i] = strips[i]->ctl;
     auto plan_all = [&]() {
-        strips_max_kernel<<<1, 32, 0, st>>>(ctls, n);
+        strips_max_kernel<<<1, 32, 0, st>>>(table);
         for (int i = 0; i < n; ++i) plan_kernel<<<1, 1, 0, st>>>(strips[i]->dd, strips[i]->ctl);
     };
-    if (cudaMemcpyAsync(ctls, hc.data(), sizeof(Control*) * (size_t)n, cudaMemcpyHostToDevice, st) != cudaSuccess)
-        rc = fail(SWE_ERR_CUDA, "copy of the strip table failed");
-    if (!rc) plan_all();
+    int rc = SWE_OK;
+    plan_all();
     const int cols = strips[0]->dd.cols;
     for (int k = 0; k < n_steps && !rc; ++k) {
         for (int i = 0; i < n; ++i) strip_step(strips[i], k, st);
@@ -1882,12 +2129,13 @@ int swe_strips_advance(const swe_domain_t* strips, int32_t n, float* const* h, f
         for (int i = 0; i + 1 < n && !rc; ++i) {
             swe_domain* L = strips[i];
             swe_domain* U = strips[i + 1];
+            const HaloRows hl = halo_rows(L), hu_ = halo_rows(U);
             for (int f = 0; f < 3 && !rc; ++f) {
-                const float* lo_row = L->ping[b][f] + (int64_t)(L->dd.upd_hi - 1) * L->ppitch;
-                const float* up_row = U->ping[b][f] + (int64_t)U->dd.upd_lo * U->ppitch;
-                if (cudaMemcpyAsync(U->ping[b][f], lo_row, sizeof(float) * cols, cudaMemcpyDeviceToDevice, st) ||
-                    cudaMemcpyAsync(L->ping[b][f] + (int64_t)(L->dd.rows - 1) * L->ppitch, up_row, sizeof(float) * cols,
-                                    cudaMemcpyDeviceToDevice, st))
+                // L's last owned row -> U's halo row below; U's first owned row -> L's halo row above.
+                if (cudaMemcpyAsync(plane_row(U, b, f, hu_.recv_below), plane_row(L, b, f, hl.send_above),
+                                    sizeof(float) * cols, cudaMemcpyDeviceToDevice, st) ||
+                    cudaMemcpyAsync(plane_row(L, b, f, hl.recv_above), plane_row(U, b, f, hu_.send_below),
+                                    sizeof(float) * cols, cudaMemcpyDeviceToDevice, st))
                     rc = fail(SWE_ERR_CUDA, "halo copy failed");
             }
         }
@@ -1895,27 +2143,54 @@ int swe_strips_advance(const swe_domain_t* strips, int32_t n, float* const* h, f
     if (!rc && cudaGetLastError() != cudaSuccess) rc = fail(SWE_ERR_CUDA, "strip step launch failed");
     for (int i = 0; i < n && !rc; ++i) rc = strip_finish(strips[i], h[i], hu[i], hv[i], pitch[i], n_steps, &results[i], st);
     cudaStreamSynchronize(st);
-    cudaFree(ctls);
     if (rc) return rc;
     for (int i = 0; i < n; ++i)
         if (results[i].status) return fail(results[i].status, "a strip stopped with an error status");
     return SWE_OK;
 }
 
+// Every rank takes the same NCCL steps in the same order, error paths
+// included: the argument checks and the set-up run first on every rank, then
+// one all-reduce of their status decides for all ranks whether to go on; every
+// later wait is bounded, and a wait that runs out aborts the communicator.
 int swe_strip_advance_nccl(swe_domain_t d, swe_comm_t comm, int32_t rank_below, int32_t rank_above, float* h,
                            float* hu, float* hv, int64_t pitch, int32_t n_steps, double t0, swe_run_result* result,
                            void* stream) {
-    if (!d || !comm || !result || n_steps < 0) return fail(SWE_ERR_INVALID, "bad strip arguments");
     const NcclApi* api = nccl_api();
     if (!api) return fail(SWE_ERR_INVALID, "NCCL (libnccl.so.2) could not be loaded");
-    if ((rank_below >= 0) != (d->dd.upd_lo == 1) || (rank_above >= 0) != (d->dd.upd_hi == d->dd.rows - 1))
-        return fail(SWE_ERR_INVALID, "neighbour ranks must match the strip's halo rows");
+    if (!comm || !comm->comm) return fail(SWE_ERR_INVALID, "no usable communicator");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    int rc = strip_begin(d, h, hu, hv, pitch, t0, n_steps, st);
+    // 1. Local checks and set-up, without returning before the agreement.
+    int local = SWE_OK;
+    std::string local_msg;
+    if (!d || !result || n_steps < 0) {
+        local = SWE_ERR_INVALID;
+        local_msg = "bad strip arguments";
+    } else if ((rank_below >= 0) != (d->dd.upd_lo == 1) || (rank_above >= 0) != (d->dd.upd_hi == d->dd.rows - 1)) {
+        local = SWE_ERR_INVALID;
+        local_msg = "neighbour ranks must match the strip's halo rows";
+    } else {
+        local = strip_begin(d, h, hu, hv, pitch, t0, n_steps, st);
+        if (local) local_msg = g_err;
+    }
+    // 2. Agreement: the largest status over all ranks.
+    *comm->status_host = local;
+    SWE_CK(cudaMemcpyAsync(comm->status_dev, comm->status_host, sizeof(int), cudaMemcpyHostToDevice, st));
+    ncclResult_t r = nccl_settle(api, comm, api->AllReduce(comm->status_dev, comm->status_dev, 1, ncclInt32, ncclMax,
+                                                           comm->comm, st));
+    if (r != ncclSuccess) return nccl_abort(api, comm, std::string("status all-reduce: ") + api->GetErrorString(r));
+    SWE_CK(cudaMemcpyAsync(comm->status_host, comm->status_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int rc = nccl_wait(api, comm, st);
     if (rc) return rc;
+    if (local) return fail(local, local_msg);
+    if (*comm->status_host) return fail(*comm->status_host, "another rank's strip arguments or set-up failed");
+    // 3. The steps.  Each NCCL call is settled; the group is always closed.
     const int cols = d->dd.cols;
+    const HaloRows hr = halo_rows(d);
     auto plan = [&]() -> int {
-        SWE_NCCL(api->AllReduce(&d->ctl->maxinv, &d->ctl->maxinv, 1, ncclFloat, ncclMax, comm->comm, st));
+        const ncclResult_t e = nccl_settle(api, comm, api->AllReduce(&d->ctl->maxinv, &d->ctl->maxinv, 1, ncclFloat,
+                                                                     ncclMax, comm->comm, st));
+        if (e != ncclSuccess) return nccl_abort(api, comm, std::string("all-reduce: ") + api->GetErrorString(e));
         plan_kernel<<<1, 1, 0, st>>>(d->dd, d->ctl);
         return SWE_OK;
     };
@@ -1925,23 +2200,31 @@ int swe_strip_advance_nccl(swe_domain_t d, swe_comm_t comm, int32_t rank_below, 
         rc = plan();
         if (rc) break;
         const int b = (k + 1) & 1;
-        SWE_NCCL(api->GroupStart());
-        for (int f = 0; f < 3; ++f) {
-            float* plane = d->ping[b][f];
+        ncclResult_t first = api->GroupStart();
+        for (int f = 0; f < 3 && first == ncclSuccess; ++f) {
+            auto keep = [&](ncclResult_t x) {
+                if (first == ncclSuccess && x != ncclSuccess && x != ncclInProgress) first = x;
+            };
             if (rank_below >= 0) {
-                SWE_NCCL(api->Send(plane + (int64_t)d->dd.upd_lo * d->ppitch, cols, ncclFloat, rank_below, comm->comm, st));
-                SWE_NCCL(api->Recv(plane, cols, ncclFloat, rank_below, comm->comm, st));
+                keep(api->Send(plane_row(d, b, f, hr.send_below), cols, ncclFloat, rank_below, comm->comm, st));
+                keep(api->Recv(plane_row(d, b, f, hr.recv_below), cols, ncclFloat, rank_below, comm->comm, st));
             }
             if (rank_above >= 0) {
-                SWE_NCCL(api->Send(plane + (int64_t)(d->dd.upd_hi - 1) * d->ppitch, cols, ncclFloat, rank_above,
-                                   comm->comm, st));
-                SWE_NCCL(api->Recv(plane + (int64_t)(d->dd.rows - 1) * d->ppitch, cols, ncclFloat, rank_above,
-                                   comm->comm, st));
+                keep(api->Send(plane_row(d, b, f, hr.send_above), cols, ncclFloat, rank_above, comm->comm, st));
+                keep(api->Recv(plane_row(d, b, f, hr.recv_above), cols, ncclFloat, rank_above, comm->comm, st));
             }
         }
-        SWE_NCCL(api->GroupEnd());
+        const ncclResult_t end = nccl_settle(api, comm, api->GroupEnd());
+        if (first == ncclSuccess) first = end;
+        if (first != ncclSuccess) {
+            rc = nccl_abort(api, comm, std::string("halo exchange: ") + api->GetErrorString(first));
+            break;
+        }
+        // Bound the wait on the other ranks every kChunk steps.
+        if ((k + 1) % kChunk == 0) rc = nccl_wait(api, comm, st);
     }
     if (!rc && cudaGetLastError() != cudaSuccess) rc = fail(SWE_ERR_CUDA, "strip step launch failed");
+    if (!rc) rc = nccl_wait(api, comm, st);
     if (!rc) rc = strip_finish(d, h, hu, hv, pitch, n_steps, result, st);
     if (rc) return rc;
     if (result->status) return fail(result->status, "the strip stopped with an error status");

@@ -73,6 +73,28 @@ def _check_local(states, shapes, device) -> None:
                 raise ValueError(f"strip states must be device float32 {shape} tensors with unit column stride")
 
 
+def agree_on_errors(err: Exception | None, world: int, group=None, device=None) -> None:
+    """Raise on every rank of ``group`` if any rank's local check failed.
+
+    Each rank passes the exception its own checks raised (or ``None``); one
+    all-reduce (max) of a flag tells every rank whether any of them failed, so
+    either all ranks go on into the collective steps or none does.  The failing
+    rank re-raises its own exception, the others a ``ValueError`` naming that
+    another rank failed.
+    """
+    import torch.distributed as dist
+
+    if world > 1:
+        flag = torch.tensor([1 if err is not None else 0], dtype=torch.int32)
+        if dist.get_backend(group) == "nccl":
+            flag = flag.to(device)
+        dist.all_reduce(flag, op=dist.ReduceOp.MAX, group=group)
+        if int(flag.item()) and err is None:
+            raise ValueError("another rank's strip arguments are invalid")
+    if err is not None:
+        raise err
+
+
 def _results(res) -> list[tuple]:
     return [(float(r.final_time_s), int(r.steps_used), dict(zip(LEDGER_KEYS, list(r.ledger)))) for r in res]
 
@@ -160,6 +182,7 @@ class NcclStrip(_StripBase):
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.rows, self.cols = np.asarray(member["bed"]).shape
         self.rank, self.world = int(rank), int(world)
+        self._group = group
         self.ranges = row_ranges(self.rows, self.world)
         lo, hi = self.ranges[self.rank]
         self._handle = self._make(member, arithmetic, lo, hi)
@@ -192,7 +215,21 @@ class NcclStrip(_StripBase):
         return split_state(SWEState(*state), self.rows, [self.ranges[self.rank]])[0]
 
     def advance_(self, local_state, n_steps: int, start_time_s: float = 0.0) -> tuple:
-        _check_local([local_state], [self.shape], self.device)
+        """``n_steps`` domain-wide steps of this rank's strip IN PLACE.
+
+        Every rank must call it with the same ``n_steps`` and ``start_time_s``.
+        The ranks first agree over the ``torch.distributed`` group that every
+        one of them has valid arguments (a rank whose check fails still takes
+        part in that agreement), so no rank enters the NCCL steps while another
+        has left; the library then agrees once more on its own set-up and
+        bounds every later wait (``SWE_NCCL_TIMEOUT_S``).
+        """
+        err = None
+        try:
+            _check_local([local_state], [self.shape], self.device)
+        except ValueError as e:
+            err = e
+        agree_on_errors(err, self.world, self._group, self.device)
         res = _lib.RunResult()
         with torch.cuda.device(self.device):
             rc = self._lib.swe_strip_advance_nccl(

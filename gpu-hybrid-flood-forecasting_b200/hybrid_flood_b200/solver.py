@@ -288,6 +288,39 @@ class B200ShallowWaterSolver:
         _lib.check(rc, "advance")
         return float(res.final_time_s), int(res.steps_used), dict(zip(LEDGER_KEYS, list(res.ledger)))
 
+    # -- device-resident stepping ------------------------------------------------
+    def resident_load(self, state, start_time_s: float = 0.0) -> None:
+        """Copy ``state`` into the solver's own device buffers and start the clock.
+
+        The reference's step loop (``numpy_solver/shallow_water_2d.py:402-412``)
+        then runs on that resident copy through :meth:`resident_steps`, without
+        the state leaving the device between calls.
+        """
+        st = _as_state(state, self.device, self.shape)
+        with torch.cuda.device(self.device):
+            rc = self._lib.swe_resident_load(self._handle, _ptr(st.h), _ptr(st.hu), _ptr(st.hv), _pitch(st.h),
+                                             float(start_time_s), _stream(self.device))
+        _lib.check(rc, "resident_load")
+
+    def resident_steps(self, n_steps: int) -> None:
+        """Enqueue ``n_steps`` CFL-limited steps of the resident state; returns at once."""
+        with torch.cuda.device(self.device):
+            rc = self._lib.swe_resident_steps(self._handle, int(n_steps), _stream(self.device))
+        _lib.check(rc, "resident_steps")
+
+    def resident_store(self, state: SWEState) -> tuple[float, int, dict]:
+        """Copy the resident state into ``state`` (device tensors); ``(time, steps since load, ledger)``."""
+        for t in state:
+            if not (isinstance(t, torch.Tensor) and t.device == self.device and t.dtype == torch.float32
+                    and tuple(t.shape) == self.shape and t.stride(-1) == 1):
+                raise ValueError("resident_store needs device float32 [rows, cols] tensors")
+        res = _lib.RunResult()
+        with torch.cuda.device(self.device):
+            rc = self._lib.swe_resident_store(self._handle, _ptr(state.h), _ptr(state.hu), _ptr(state.hv),
+                                              _pitch(state.h), ctypes.byref(res), _stream(self.device))
+        _lib.check(rc, "resident_store")
+        return float(res.final_time_s), int(res.steps_used), dict(zip(LEDGER_KEYS, list(res.ledger)))
+
     def advance_to_(self, state: SWEState, start_time_s: float, target_time_s: float,
                     max_steps: int, dt_log: torch.Tensor | None = None) -> tuple[float, int, dict]:
         """Advance ``state`` IN PLACE from ``start_time_s`` to ``target_time_s``.

@@ -128,6 +128,26 @@ int swe_run(swe_domain_t d, const float *h0, const float *hu0, const float *hv0,
 int swe_advance(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, int32_t n_steps,
                 double start_s, swe_run_result *result, void *stream);
 
+/* Device-resident stepping: the reference's step loop
+ * (`state = finite_volume_step(state, params, compute_cfl_dt(state), t)`,
+ * numpy_solver/shallow_water_2d.py:402-412) with the state kept in the
+ * domain's own buffers between calls, so that a caller can advance in pieces
+ * without copying the state in and out each time.
+ *   swe_resident_load   copies (h, hu, hv) in and starts the float64 clock at
+ *                       start_s (the initial CFL reduction is enqueued);
+ *   swe_resident_steps  enqueues n_steps CFL-limited steps and returns without
+ *                       waiting (whole 32-step CUDA graphs where possible);
+ *   swe_resident_store  copies the current state out and reports the clock,
+ *                       the steps taken since the load and the FP64 ledger
+ *                       (it synchronises the stream).
+ * Any other run on the domain (swe_run, swe_advance, swe_advance_to, an
+ * ensemble or strip advance) ends the resident state. */
+int swe_resident_load(swe_domain_t d, const float *h, const float *hu, const float *hv, int64_t pitch,
+                      double start_s, void *stream);
+int swe_resident_steps(swe_domain_t d, int32_t n_steps, void *stream);
+int swe_resident_store(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch,
+                       swe_run_result *result, void *stream);
+
 /* Number of kernel launches the last swe_run/swe_advance on this domain enqueued. */
 int64_t swe_last_launch_count(swe_domain_t d);
 

@@ -135,3 +135,42 @@ def test_gloo_strips_equal_the_undivided_oracle(tmp_path, world):
         np.testing.assert_array_equal(parts[r]["dts"], np.array(dts))
     for q, name in enumerate(("h", "hu", "hv")):
         np.testing.assert_array_equal(np.concatenate([x[name] for x in parts]), st[q])
+
+
+def _agree_worker(rank, world, port, out_dir, failing):
+    from hybrid_flood_b200.decomposition import agree_on_errors
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=30))
+    try:
+        err = ValueError(f"rank {rank}: bad strip state") if rank in failing else None
+        try:
+            agree_on_errors(err, world)
+            outcome = "ok"
+        except ValueError as e:
+            outcome = str(e)
+        # every rank is still in step: one more collective completes
+        t = torch.ones(1)
+        dist.all_reduce(t)
+        with open(os.path.join(out_dir, f"agree{rank}.json"), "w") as f:
+            json.dump({"outcome": outcome, "after": float(t.item())}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("failing", [(), (1,), (0, 2)])
+def test_ranks_agree_before_the_collective_steps(tmp_path, failing):
+    """A rank whose argument check fails does not leave the others waiting in
+    NCCL: every rank learns of the failure from one all-reduce and raises, and
+    all ranks stay in step for the next collective."""
+    world = 3
+    mp.spawn(_agree_worker, args=(world, _port(), str(tmp_path), failing), nprocs=world, join=True)
+    out = [json.loads((tmp_path / f"agree{r}.json").read_text()) for r in range(world)]
+    for r, o in enumerate(out):
+        assert o["after"] == world
+        if not failing:
+            assert o["outcome"] == "ok"
+        elif r in failing:
+            assert o["outcome"] == f"rank {r}: bad strip state"
+        else:
+            assert o["outcome"] == "another rank's strip arguments are invalid"

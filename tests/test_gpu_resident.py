@@ -1,0 +1,81 @@
+"""Device-resident stepping and the captured step graphs (GPU, through the C ABI).
+
+The resident run is the reference's step loop (``numpy_solver/shallow_water_2d.py:402-412``)
+on a state that stays in the solver's buffers: advancing it in pieces of any
+length must give the same state, clock, step count and ledger, bit for bit, as
+one ``swe_advance`` over the whole count, whether the pieces are replayed from a
+32-step CUDA graph or launched one step at a time.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(arith):
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver
+    from hybrid_flood_b200.workloads import street_depth, urban
+
+    w = urban(192, 320, seed=5)
+    s = B200ShallowWaterSolver(w.bed, w.manning_n, w.domain_mask, **w.solver_kwargs(), arithmetic=arith)
+    return s, s.initial_state(depth_m=street_depth(w))
+
+
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+def test_resident_pieces_equal_one_advance(cuda_device, arith):
+    s, init = _case(arith)
+    pieces = (7, 32, 33, 1, 64, 3)  # odd starts, whole graphs, graph + remainder
+    total = sum(pieces)
+    ref, t_ref, n_ref, led_ref = s.advance(init, total, 2.5)
+    s.resident_load(init, 2.5)
+    for k in pieces:
+        s.resident_steps(k)
+    out = type(init)(*(torch.empty_like(t) for t in init))
+    t, n, led = s.resident_store(out)
+    assert n == n_ref == total
+    assert t == t_ref
+    assert led == led_ref
+    for a, b in zip(out, ref):
+        assert torch.equal(a, b)
+    # the store does not end the resident run: more steps continue from it
+    s.resident_steps(5)
+    t2, n2, _ = s.resident_store(out)
+    assert n2 == total + 5 and t2 > t
+
+
+def test_resident_run_is_ended_by_other_runs(cuda_device):
+    s, init = _case("fast")
+    out = type(init)(*(torch.empty_like(t) for t in init))
+    with pytest.raises(ValueError, match="resident"):
+        s.resident_steps(1)
+    s.resident_load(init)
+    s.resident_steps(2)
+    s.advance(init, 3)  # any other run replaces the resident state
+    with pytest.raises(ValueError, match="resident"):
+        s.resident_store(out)
+
+
+def test_run_with_graph_chunks_matches_the_oracle_step_count(cuda_device):
+    """swe_run replays 32-step graphs between its completion polls: a run of a
+    few hundred steps still stops exactly at its output times."""
+    from conftest import rel_l2
+    from oracle import cport
+    from oracle import swe_numpy as O
+    from hybrid_flood_b200.workloads import street_depth, urban
+
+    w = urban(96, 160, seed=8)
+    p = O.make_params(w.bed, w.manning_n, w.domain_mask, **w.solver_kwargs())
+    init = O.initial_state(p, depth_m=street_depth(w))
+    times = np.asarray([0.0, 20.0, 45.0, 90.0], np.float32)
+    want = cport.Domain(p).run(init, times)
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver
+
+    s = B200ShallowWaterSolver(w.bed, w.manning_n, w.domain_mask, **w.solver_kwargs(), arithmetic="exact")
+    got = s.run(list(init), times)
+    assert got.steps_used == want[2] and got.steps_used > 64
+    for k in range(len(times)):
+        assert rel_l2(got.states.h[k].cpu().numpy(), want[0][k, 0]) < 1e-5

@@ -65,6 +65,48 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls(cuda_device):
     assert want[0] != want[1]
 
 
+def test_noalloc_padded_pitch_matches_allocating_entry_point(cuda_device):
+    """State planes whose row pitch exceeds the column count (views into wider
+    buffers): the kernel reads the state at the pitch and the mask densely, and
+    the result equals the allocating entry point's on the same views, twice."""
+    from hybrid_flood_b200 import _lib
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver, SWEState
+    from hybrid_flood_b200.workloads import urban
+
+    rows, cols, pad = 200, 300, 37
+    w = urban(rows, cols, seed=4)
+    mask = np.ones((rows, cols), dtype=bool)
+    mask[20:90, 5:40] = False
+    kw = w.solver_kwargs()
+    s = B200ShallowWaterSolver(w.bed, w.manning_n, mask, **kw, arithmetic="exact")
+    rng = np.random.default_rng(17)
+    lib = _lib.load()
+    mask_dev = torch.from_numpy(mask.astype(np.uint8)).to(cuda_device)
+    out = torch.full((1,), -1.0, dtype=torch.float32, device=cuda_device)
+    got, want = [], []
+    for depth, speed in ((0.3, 2.0), (0.02, 0.1)):
+        dense = s.initial_state(depth_m=rng.uniform(0.0, depth, (rows, cols)).astype(np.float32),
+                                x_velocity_m_s=rng.normal(0.0, speed, (rows, cols)).astype(np.float32),
+                                y_velocity_m_s=rng.normal(0.0, speed, (rows, cols)).astype(np.float32))
+        # padding filled with values that would dominate the maximum if read
+        wide = [torch.full((rows, cols + pad), 50.0, device=cuda_device) for _ in range(3)]
+        views = []
+        for big, a in zip(wide, dense):
+            v = big[:, :cols]
+            v.copy_(a)
+            views.append(v)
+        st = SWEState(*views)
+        assert st.h.stride(0) == cols + pad
+        rc = _noalloc(lib, st, mask_dev, rows, cols, out, g=kw["gravity_m_s2"],
+                      dry=kw["dry_tolerance_m"], dx=kw["resolution_m"])
+        _lib.check(rc, "swe_max_inverse_dt_noalloc")
+        torch.cuda.synchronize()
+        got.append(float(out.item()))
+        want.append(s.max_inverse_dt(st))
+    assert got == want
+    assert want[0] != want[1]
+
+
 def test_noalloc_rejects_grids_above_its_limit(cuda_device):
     from hybrid_flood_b200 import _lib
 
