@@ -298,6 +298,30 @@ def _parity(args, w, depth, dev) -> dict:
     return out
 
 
+def _device_setup(ws, arith: str, dev) -> dict:
+    """Time generating the same members' fields on the device (their own seeded
+    draws, hybrid_flood_b200.generators) and creating the ensemble from them."""
+    import torch
+
+    from hybrid_flood_b200.ensemble import B200Ensemble
+    from hybrid_flood_b200.generators import member_fields, urban_device
+
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    mems = [member_fields(urban_device(w.shape[0], w.shape[1], seed=int(w.meta["seed"]),
+                                       rain_scale=float(w.meta["rain_scale"]), n_scale=float(w.meta["n_scale"]),
+                                       device=dev)) for w in ws]
+    torch.cuda.synchronize(dev)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ens = B200Ensemble(mems, arithmetic=arith, device=dev)
+    torch.cuda.synchronize(dev)
+    create_s = time.perf_counter() - t0
+    del ens, mems
+    return {"device_generate_s": gen_s, "device_fields_ensemble_create_s": create_s,
+            "members": len(ws), "cells": int(sum(w.bed.size for w in ws))}
+
+
 def _ensemble(args, dev, rank: int, world: int):
     """Batched 64-member ensemble vs the same members run one by one (plain path).
 
@@ -314,13 +338,21 @@ def _ensemble(args, dev, rank: int, world: int):
     from hybrid_flood_b200.solver import B200ShallowWaterSolver, ledger_error
     from hybrid_flood_b200.workloads import as_member, ensemble_members, street_depth
 
+    t0 = time.perf_counter()
     ws_all = ensemble_members(args.ensemble_members)
+    host_gen_s = time.perf_counter() - t0
     cells_all = [w.shape[0] * w.shape[1] for w in ws_all]
     mine = shard_members(cells_all, world)[rank]
     ws = [ws_all[i] for i in mine]
     members = [as_member(w) for w in ws]
     depths = [street_depth(w) for w in ws]
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
     ens = B200Ensemble(members, arithmetic=args.arith, device=dev)
+    torch.cuda.synchronize(dev)
+    host_create_s = time.perf_counter() - t0
+    setup = _device_setup(ws, args.arith, dev)
+    setup.update({"host_numpy_generate_s": host_gen_s, "host_fields_ensemble_create_s": host_create_s})
     states = ens.initial_states(depths)
     ens.advance_(states, 50)  # spin-up
     tune_states = [type(s)(*(t.clone() for t in s)) for s in states]
@@ -336,7 +368,10 @@ def _ensemble(args, dev, rank: int, world: int):
     ms = max_over_ranks(ms)
     cells = sum(cells_all)
     value = cells * n / (ms / 1e3)
-    worst_ledger = max_over_ranks(max(ledger_error(r[2]) for r in res))
+    errs = [ledger_error(r[2]) for r in res]
+    worst_ledger = max_over_ranks(max(errs))
+    worst_member = {"index": int(mine[int(np.argmax(errs))]), "steps": int(res[int(np.argmax(errs))][1]),
+                    "shape": list(ws[int(np.argmax(errs))].shape)}
     # Plain path, member after member, same steps (each member its own solver, resident state).
     solvers = [B200ShallowWaterSolver(m["bed"], m["manning_n"], m["domain_mask"],
                                       **{k: v for k, v in m.items() if k not in ("bed", "manning_n", "domain_mask")},
@@ -364,7 +399,8 @@ def _ensemble(args, dev, rank: int, world: int):
         "roofline_frac": BYTES_PER_CELL * value / world / 1e9 / peak, "peak_kind": kind,
         "plain_sequential_value": plain_value, "speedup_vs_plain_sequential": value / plain_value,
         "timing": "both arms: CUDA events around the step launches only (states loaded beforehand)",
-        "ledger_rel_error_max": worst_ledger, "gpu_launches": ens.last_launch_count(),
+        "ledger_rel_error_max": worst_ledger, "ledger_worst_member": worst_member,
+        "gpu_launches": ens.last_launch_count(), "setup": setup,
         "workload": f"{len(ws_all)} urban members from {{256^2, 512^2, 1024^2, 768x1536}}, dx=1m, "
                     "rain x LogNormal(0.4), n x U(0.8,1.2), seeds 1000+m",
     }

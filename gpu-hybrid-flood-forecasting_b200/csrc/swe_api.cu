@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -26,6 +27,7 @@
 #include "swe_adjoint.cuh"
 #include "swe_hybrid.cuh"
 #include "swe_nn.cuh"
+#include "swe_gen.cuh"
 
 using namespace swe;
 
@@ -136,6 +138,35 @@ struct swe_domain {
 
 namespace {
 
+// Step kernels are launched with programmatic stream serialisation, so that a
+// step's launch overlaps the end of the previous step (the kernels wait for
+// their predecessor with griddepcontrol.wait before touching memory).
+// SWE_PDL=0 turns it off.
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("SWE_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+cudaLaunchConfig_t pdl_config(int blocks, cudaStream_t st) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3((unsigned)kThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    return cfg;
+}
+
+void attach_pdl(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr) {
+    if (!pdl_enabled()) return;
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+}
+
 // Kernel instance for (vector width, arithmetic, run mode, masked) chosen at run time.
 // V = 2 runs the paired-lane kernel; V = 1 (pitches or pointers that are not
 // 8-byte aligned) the scalar one.
@@ -148,10 +179,13 @@ struct StepK {
             return reinterpret_cast<const void*>(&step_kernel<V, M, kThreads, RUN, MASKED>);
     }
     static void launch(int blocks, const StepLaunch& sl, cudaStream_t st) {
+        cudaLaunchConfig_t cfg = pdl_config(blocks, st);
+        cudaLaunchAttribute attr[1];
+        attach_pdl(cfg, attr);
         if constexpr (V == 2)
-            step_kernel_pair<M, kThreads, RUN, MASKED><<<blocks, kThreads, 0, st>>>(sl);
+            cudaLaunchKernelEx(&cfg, step_kernel_pair<M, kThreads, RUN, MASKED>, sl);
         else
-            step_kernel<V, M, kThreads, RUN, MASKED><<<blocks, kThreads, 0, st>>>(sl);
+            cudaLaunchKernelEx(&cfg, step_kernel<V, M, kThreads, RUN, MASKED>, sl);
     }
 };
 
@@ -540,14 +574,25 @@ struct swe_ensemble {
     unsigned* done_counter = nullptr;       // device: members finished in advance_to
     unsigned* done_host = nullptr;          // pinned: two polled copies of it
     cudaEvent_t poll_ev[2] = {nullptr, nullptr};
+    // Member table in the kernel's parameter space (up to kEnsParamMembers
+    // members; SWE_ENS_PARAM_TABLE=0 keeps the table in global memory).
+    std::unique_ptr<EnsParams> params;
 };
 
 namespace {
 
 template <class M, bool MASKED>
 void ens_launch_t(const swe_ensemble* e, int parity, cudaStream_t st) {
-    ensemble_step_kernel<M, kThreads, MASKED><<<e->grid, kThreads, 0, st>>>(e->members_dev, e->items_dev,
-                                                                            e->n_items, parity);
+    cudaLaunchConfig_t cfg = pdl_config(e->grid, st);
+    cudaLaunchAttribute attr[1];
+    attach_pdl(cfg, attr);
+    if (e->params) {
+        e->params->parity = parity;
+        cudaLaunchKernelEx(&cfg, ensemble_step_kernel_p<M, kThreads, MASKED>, *e->params);
+    } else {
+        cudaLaunchKernelEx(&cfg, ensemble_step_kernel<M, kThreads, MASKED>, (const MemberDev*)e->members_dev,
+                           (const int2*)e->items_dev, e->n_items, parity);
+    }
 }
 
 void ens_launch(const swe_ensemble* e, int parity, cudaStream_t st) {
@@ -560,7 +605,14 @@ void ens_launch(const swe_ensemble* e, int parity, cudaStream_t st) {
 
 int ens_occupancy(const swe_ensemble* e) {
     const void* fn = nullptr;
-    if (e->arith == SWE_ARITH_FAST)
+    if (e->params) {
+        if (e->arith == SWE_ARITH_FAST)
+            fn = e->masked ? reinterpret_cast<const void*>(&ensemble_step_kernel_p<FastMath, kThreads, true>)
+                           : reinterpret_cast<const void*>(&ensemble_step_kernel_p<FastMath, kThreads, false>);
+        else
+            fn = e->masked ? reinterpret_cast<const void*>(&ensemble_step_kernel_p<ExactMath, kThreads, true>)
+                           : reinterpret_cast<const void*>(&ensemble_step_kernel_p<ExactMath, kThreads, false>);
+    } else if (e->arith == SWE_ARITH_FAST)
         fn = e->masked ? reinterpret_cast<const void*>(&ensemble_step_kernel<FastMath, kThreads, true>)
                        : reinterpret_cast<const void*>(&ensemble_step_kernel<FastMath, kThreads, false>);
     else
@@ -613,6 +665,21 @@ int ens_rebuild(swe_ensemble* e) {
     SWE_CK(cudaMemcpy(e->members_dev, md.data(), sizeof(MemberDev) * md.size(), cudaMemcpyHostToDevice));
     SWE_CK(cudaMemcpy(e->items_dev, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice));
     e->n_items = (int)items.size();
+    const char* pt = std::getenv("SWE_ENS_PARAM_TABLE");
+    e->params.reset();
+    if ((int)md.size() <= kEnsParamMembers && !(pt && pt[0] == '0')) {
+        e->params.reset(new EnsParams());
+        std::memset(e->params.get(), 0, sizeof(EnsParams));
+        int b = 0;
+        for (size_t m = 0; m < md.size(); ++m) {
+            e->params->m[m] = md[m];
+            e->params->cta_begin[m] = b;
+            b += md[m].ncta;
+        }
+        e->params->cta_begin[md.size()] = b;
+        e->params->n_members = (int)md.size();
+        e->params->n_items = b;
+    }
     e->grid = std::max(1, std::min(e->n_items, ens_occupancy(e) * e->sms));
     if (e->graph) {
         cudaGraphExecDestroy(e->graph);
@@ -888,6 +955,9 @@ int swe_domain_create(const swe_domain_desc* desc, swe_domain_t* out) {
     }
     const int rows = q.rows, cols = q.cols;
     const int64_t pitch = round_up(cols, 128);
+    // The step kernels address a plane with 32-bit element offsets.
+    if ((int64_t)(rows + 2) * pitch >= (int64_t(1) << 31))
+        return fail(SWE_ERR_INVALID, "domain too large: a plane must hold fewer than 2^31 elements");
     const size_t plane = sizeof(float) * (size_t)pitch * rows;
     const size_t n = (size_t)rows * cols;
     auto bail = [&](int code) { free_domain(d); return code; };
@@ -1102,6 +1172,8 @@ int swe_step(swe_domain_t d, const float* h, const float* hu, const float* hv, i
     for (auto a : ins)
         for (auto b : outs)
             if (a == b) return fail(SWE_ERR_INVALID, "step outputs must not alias its inputs");
+    if ((int64_t)d->dd.rows * std::max(pitch_in, pitch_out) >= (int64_t(1) << 31))
+        return fail(SWE_ERR_INVALID, "state planes must hold fewer than 2^31 elements");
     const void* all[6] = {h, hu, hv, h_out, hu_out, hv_out};
     const int V = choose_vec(all, 6, pitch_in, pitch_out);
     const Plan pl = make_plan(d, V, false);
@@ -1787,6 +1859,154 @@ int swe_last_step_time(swe_domain_t d, double* ms, int64_t* step_launches) {
     return SWE_OK;
 }
 
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Device generators of the synthetic inputs (swe_generate_*)
+// ---------------------------------------------------------------------------
+namespace {
+
+// Device scratch that frees itself (the generators are set-up calls).
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    ~DevBuf() { cudaFree(p); }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * std::max<size_t>(n, 1)); }
+};
+
+int gen_blocks(int64_t work, int sms) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)sms * 8));
+}
+
+int device_sms() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+}  // namespace
+
+extern "C" {
+
+int swe_generate_urban(const swe_urban_desc* q, float* bed, float* manning_n, uint8_t* block_mask,
+                       int32_t* blocks_used, void* stream) {
+    if (!q || !bed || !manning_n) return fail(SWE_ERR_INVALID, "null argument");
+    if (q->rows < 1 || q->cols < 1) return fail(SWE_ERR_INVALID, "rows and cols must be >= 1");
+    if (!(q->dx > 0)) return fail(SWE_ERR_INVALID, "dx must be positive");
+    if (!(q->coverage >= 0.0 && q->coverage <= 1.0)) return fail(SWE_ERR_INVALID, "coverage must lie in [0, 1]");
+    if (q->n_rects < 0 || (q->n_rects > 0 && !q->rects)) return fail(SWE_ERR_INVALID, "bad rectangle list");
+    if (q->n_rects == 0 && (q->min_side < 1 || q->max_side < q->min_side))
+        return fail(SWE_ERR_INVALID, "need 1 <= min_side <= max_side");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int rows = q->rows, cols = q->cols, sms = device_sms();
+    const int64_t cells = (int64_t)rows * cols;
+    const double target = q->coverage * (double)cells;
+    DevBuf<int> first;
+    SWE_CK(first.alloc((size_t)cells));
+    int n_blocks = 0;
+    // Drawn rectangles: a first batch about twice the expected need, doubled until it reaches the target.
+    const double side = 0.5 * (q->min_side + q->max_side);
+    int n = q->n_rects > 0 ? q->n_rects
+                           : (int)std::min<double>(1 << 30, 2.0 * -std::log(std::max(1.0 - q->coverage, 1e-6)) *
+                                                                (double)cells / (side * side) + 256.0);
+    for (;;) {
+        DevBuf<Rect> rects;
+        DevBuf<int> counts;
+        SWE_CK(rects.alloc((size_t)n));
+        SWE_CK(counts.alloc((size_t)n));
+        if (q->n_rects > 0) {
+            std::vector<Rect> hr((size_t)n);
+            for (int i = 0; i < n; ++i) {
+                hr[i] = Rect{q->rects[4 * i], q->rects[4 * i + 1], q->rects[4 * i + 2], q->rects[4 * i + 3]};
+                if (hr[i].r0 < 0 || hr[i].c0 < 0 || hr[i].h < 0 || hr[i].w < 0)
+                    return fail(SWE_ERR_INVALID, "rectangles need non-negative corners and sides");
+            }
+            SWE_CK(cudaMemcpyAsync(rects.p, hr.data(), sizeof(Rect) * (size_t)n, cudaMemcpyHostToDevice, st));
+        } else {
+            gen_rects_kernel<<<(n + 255) / 256, 256, 0, st>>>(q->seed, n, rows, cols, q->min_side, q->max_side, rects.p);
+        }
+        SWE_CK(cudaMemsetAsync(first.p, 0x7f, sizeof(int) * (size_t)cells, st));  // 0x7f7f7f7f: no rectangle yet
+        SWE_CK(cudaMemsetAsync(counts.p, 0, sizeof(int) * (size_t)n, st));
+        rasterize_rects_kernel<<<std::min(n, sms * 16), 256, 0, st>>>(rects.p, n, rows, cols, first.p);
+        first_histogram_kernel<<<gen_blocks(cells, sms), 256, 0, st>>>(first.p, cells, n, counts.p);
+        SWE_CK(cudaGetLastError());
+        std::vector<int> hc((size_t)n);
+        SWE_CK(cudaMemcpyAsync(hc.data(), counts.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
+        SWE_CK(cudaStreamSynchronize(st));
+        // The sequential rule: rectangles are added while the covered cells stay below the target.
+        int64_t covered = 0;
+        int k = 0;
+        while (k < n && (double)covered < target) covered += hc[(size_t)k++];
+        if ((double)covered >= target || q->n_rects > 0 || n >= (1 << 29)) {
+            n_blocks = k;
+            break;
+        }
+        n *= 2;
+    }
+    urban_fields_kernel<<<gen_blocks(cells, sms), 256, 0, st>>>(first.p, n_blocks, rows, cols, q->dx, q->slope,
+                                                              q->block_raise_m, q->street_offset_m, q->n_block,
+                                                              q->n_street, q->n_scale, bed, manning_n, block_mask);
+    SWE_CK(cudaGetLastError());
+    SWE_CK(cudaStreamSynchronize(st));  // the scratch is freed on return
+    if (blocks_used) *blocks_used = n_blocks;
+    return SWE_OK;
+}
+
+int swe_generate_gamma_hyetograph(int32_t n, double step_s, double shape_k, double scale, double to_m_s,
+                                  uint64_t seed, float* times, float* rates, void* stream) {
+    if (n < 1 || !times || !rates) return fail(SWE_ERR_INVALID, "need n >= 1 and output buffers");
+    if (!(shape_k > 0) || !(scale > 0)) return fail(SWE_ERR_INVALID, "Gamma shape and scale must be positive");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    gamma_hyetograph_kernel<<<(n + 127) / 128, 128, 0, st>>>(seed, n, step_s, shape_k, scale, to_m_s, times, rates);
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
+int swe_generate_lognormal_field(int32_t rows, int32_t cols, double median, double sigma_log, int32_t smooth_cells,
+                                 uint64_t seed, const double* noise, float* out, void* stream) {
+    if (rows < 1 || cols < 1 || !out) return fail(SWE_ERR_INVALID, "bad field arguments");
+    if (!(median > 0) || !(sigma_log >= 0)) return fail(SWE_ERR_INVALID, "median must be > 0 and sigma_log >= 0");
+    if (smooth_cells < 1) return fail(SWE_ERR_INVALID, "smooth_cells must be >= 1");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t cells = (int64_t)rows * cols;
+    const int sms = device_sms();
+    const int radius = smooth_cells / 2;
+    // Gaussian taps of width smooth_cells (sigma = smooth_cells / 6), normalised to sum 1.
+    std::vector<double> taps((size_t)(2 * radius + 1));
+    double tsum = 0.0;
+    const double sig = smooth_cells / 6.0;
+    for (int t = -radius; t <= radius; ++t) {
+        const double x = (double)t / sig;
+        taps[(size_t)(t + radius)] = std::exp(-0.5 * x * x);
+        tsum += taps[(size_t)(t + radius)];
+    }
+    for (auto& v : taps) v /= tsum;
+    DevBuf<double> a, b, dtaps, partials, sums;
+    SWE_CK(a.alloc((size_t)cells));
+    SWE_CK(b.alloc((size_t)cells));
+    SWE_CK(dtaps.alloc(taps.size()));
+    SWE_CK(partials.alloc(kGenSumBlocks));
+    SWE_CK(sums.alloc(2));
+    SWE_CK(cudaMemcpyAsync(dtaps.p, taps.data(), sizeof(double) * taps.size(), cudaMemcpyHostToDevice, st));
+    const double* src = noise;
+    if (!src) {
+        normal_field_kernel<<<gen_blocks(cells, sms), 256, 0, st>>>(seed, cells, a.p);
+        src = a.p;
+    }
+    smooth_pass_kernel<1><<<gen_blocks(cells, sms), 256, 0, st>>>(src, b.p, rows, cols, dtaps.p, radius);
+    smooth_pass_kernel<0><<<gen_blocks(cells, sms), 256, 0, st>>>(b.p, a.p, rows, cols, dtaps.p, radius);
+    // Two-pass moments: the mean, then the squared deviations from it.
+    block_sums_kernel<256><<<kGenSumBlocks, 256, 0, st>>>(a.p, cells, nullptr, partials.p);
+    fold_sums_kernel<<<1, 32, 0, st>>>(partials.p, kGenSumBlocks, sums.p);
+    block_sums_kernel<256><<<kGenSumBlocks, 256, 0, st>>>(a.p, cells, sums.p, partials.p);
+    fold_sums_kernel<<<1, 32, 0, st>>>(partials.p, kGenSumBlocks, sums.p + 1);
+    lognormal_finish_kernel<<<gen_blocks(cells, sms), 256, 0, st>>>(a.p, cells, sums.p, median, sigma_log, out);
+    SWE_CK(cudaGetLastError());
+    SWE_CK(cudaStreamSynchronize(st));  // the scratch is freed on return
+    return SWE_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Row strips of one domain (domain decomposition across GPUs)

@@ -343,6 +343,17 @@ __device__ inline void plan_next(const DomainDev& d, Control& c) {
     c.snap = c.out_h ? c.reach : -1;
 }
 
+// Programmatic dependent launch: a step kernel launched with the programmatic
+// stream-serialisation attribute may be scheduled while the previous step is
+// still running.  It lets its own successor launch at once and then waits,
+// before it reads or writes anything, until the previous grid has completed
+// and its memory is visible (a hardware wait, not a spin).  Launched without
+// the attribute both instructions do nothing.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
@@ -467,6 +478,10 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
         vol += s_sum[0][w]; rain += s_sum[1][w]; outflow += s_sum[2][w];
         clip += s_sum[3][w]; mask += s_sum[4][w];
     }
+    // A NaN volume means a non-finite state somewhere (the paired march folds
+    // its non-finite inverse dts into the volume partials): report it as a NaN
+    // CFL maximum, the form plan_next tests.
+    if (!(vol == vol)) mx = __int_as_float(0x7fffffff);
     Control c = *ctl;
     const double area = d.dx * d.dy;
     if (init) {
@@ -544,6 +559,7 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
     __shared__ float s_left[NW][3][kBatch];
     __shared__ float s_right[NW][7][kBatch];
 
+    pdl_enter();
     const DomainDev& d = p.d;
     const Consts& k = d.k;
     constexpr bool run = RUN;

@@ -102,7 +102,9 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
         const int rr = min(max(q, 0), d.rows - 1);
         const int sz = qi < nq ? csize : 0;
         const int slot = qi & (kRing - 1);
-        const int64_t so = (int64_t)rr * in.pitch + ccol, zo = (int64_t)rr * d.spitch + ccol;
+        // 32-bit element offsets: planes hold fewer than 2^31 elements (checked on the host).
+        const uint32_t so = (uint32_t)rr * (uint32_t)in.pitch + (uint32_t)ccol;
+        const uint32_t zo = (uint32_t)rr * (uint32_t)d.spitch + (uint32_t)ccol;
         cp_async_8z(&sm.ring[slot][0][lane], in.h + so, sz);
         cp_async_8z(&sm.ring[slot][1][lane], in.hu + so, sz);
         cp_async_8z(&sm.ring[slot][2][lane], in.hv + so, sz);
@@ -136,10 +138,13 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
             }
             __syncwarp();  // every lane has read before any slot is refilled
         }
-        const float gs = ((q < 0 && d.bnd[2] == 0) || (q >= d.rows && d.bnd[3] == 0)) ? -1.f : 1.f;
         c.h = fv[0];
         c.hu = fv[1];
-        c.hv = A::mul(fv[2], splat(gs));
+        c.hv = fv[2];
+        // Ghost rows (q is the same on every lane): a reflective edge mirrors hv.
+        if (q < 0 || q >= d.rows) {
+            if ((q < 0 ? d.bnd[2] : d.bnd[3]) == 0) c.hv = neg(c.hv);
+        }
         c.z = fv[3];
         c.nm = fv[4];
         set_vel_t<M>(c, kp);
@@ -280,23 +285,28 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
         o.hu = sel(wet, qx, kp.zero);
         o.hv = sel(wet, qy, kp.zero);
         if constexpr (RUN) {
-            CellT<float2> nc;
-            nc.h = o.h;
-            nc.hu = o.hu;
-            nc.hv = o.hv;
-            set_vel_t<M>(nc, kp);
             const float2 w = A::sqrt(A::mul(kp.g, o.h));
             float2 inv;
             if constexpr (A::kExact) {
+                CellT<float2> nc;
+                nc.h = o.h;
+                nc.hu = o.hu;
+                nc.hv = o.hv;
+                set_vel_t<M>(nc, kp);
                 inv = A::add(A::div(A::add(vabs(nc.u), w), dx2), A::div(A::add(vabs(nc.v), w), dy2));
             } else {
-                inv = A::fma(A::add(vabs(nc.u), w), rdx2, A::mul(A::add(vabs(nc.v), w), rdy2));
+                // The new momenta are zero wherever h <= dry, so 1/max(h, dry) gives the
+                // same velocities as the dry-cell rule of the reference.
+                const float2 rh = A::rcp(vmax(o.h, kp.dry));
+                inv = A::fma(A::add(vabs(A::mul(o.hu, rh)), w), rdx2, A::mul(A::add(vabs(A::mul(o.hv, rh)), w), rdy2));
             }
             // Inactive cells have h = hu = hv = 0 and so inv = 0; lanes past the edge are masked.
             inv = A::mul(inv, vmask);
-            maxinv = nan_max(maxinv, inv.x);
-            maxinv = nan_max(maxinv, inv.y);
-            lg.vol = lfma(o.h, vmask, lg.vol);
+            // Maximum without the NaN test per cell: a NaN or infinite inverse dt
+            // turns the float volume partial into NaN (0 * NaN, 0 * inf), and the
+            // fold reports the step as non-finite.
+            maxinv = fmaxf(maxinv, fmaxf(inv.x, inv.y));
+            lg.vol = lfma(inv, kp.zero, lfma(o.h, vmask, lg.vol));
             if (d.mult != nullptr) lg.rain = lfma(rain, vmask, lg.rain);
             lg.clip = lfma(neg(vmin(u0, kp.zero)), vmask, lg.clip);
             if constexpr (MASKED) {
@@ -308,7 +318,7 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
         return o;
     };
     auto store = [&](int r, const Row& o) {
-        const int64_t so = (int64_t)r * out.pitch + c0;
+        const uint32_t so = (uint32_t)r * (uint32_t)out.pitch + (uint32_t)c0;
         if (valid.y) {
             *reinterpret_cast<float2*>(out.h + so) = o.h;
             *reinterpret_cast<float2*>(out.hu + so) = o.hu;
@@ -368,8 +378,7 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
         const XF x = xfaces(cur, j);
         const Row o = update(r, cur, yT0, yT1, yT2, fy.f0, fy.f1, A::add(fy.f2, fy.corr_lo), x);
         if constexpr (RUN) {
-            const float top = r == d.rows - 1 ? 1.f : 0.f;
-            lg.out_y = lfma(fy.f0, __fmul2_rn(vmask, splat(top)), lg.out_y);
+            if (r == d.rows - 1) lg.out_y = lfma(fy.f0, vmask, lg.out_y);
         }
         yT0 = fy.f0;
         yT1 = fy.f1;
@@ -404,6 +413,7 @@ template <class M, int THREADS, bool RUN, bool MASKED>
 __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(const StepLaunch p) {
     constexpr int NW = THREADS / kWarp;
     __shared__ WarpSmem s_warp[NW];
+    pdl_enter();
     const DomainDev& d = p.d;
     StepScalars s = p.s;
     int snap = -1;
@@ -471,6 +481,7 @@ ensemble_step_kernel(const MemberDev* __restrict__ members, const int2* __restri
     constexpr int NW = THREADS / kWarp;
     __shared__ WarpSmem s_warp[NW];
     __shared__ MemberDev s_md;
+    pdl_enter();
     const int wib = threadIdx.x >> 5;
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const int2 item = items[it];
@@ -503,6 +514,62 @@ ensemble_step_kernel(const MemberDev* __restrict__ members, const int2* __restri
         a.clip = acc.clip;
         a.mask = acc.mask;
         finish_run_step<THREADS>(md.d, md.ctl, md.parts, a, false, item.y, md.ncta);
+    }
+}
+
+// The same persistent step with the member table in the kernel's parameter
+// space (ensembles of up to kEnsParamMembers members).  A CTA's member index
+// and every member field it reads are then uniform values of constant memory,
+// which the march reads as operands instead of holding them in registers.
+// Work items are numbered member after member; cta_begin[m] is member m's
+// first item, so a CTA finds its item's member by walking forward (its items
+// ascend).
+constexpr int kEnsParamMembers = 96;
+struct EnsParams {
+    MemberDev m[kEnsParamMembers];
+    int cta_begin[kEnsParamMembers + 1];
+    int n_members, n_items, parity;
+};
+
+template <class M, int THREADS, bool MASKED>
+__global__ void __launch_bounds__(THREADS, SWE_ENS_MINBLOCKS)
+ensemble_step_kernel_p(const __grid_constant__ EnsParams p) {
+    constexpr int NW = THREADS / kWarp;
+    __shared__ WarpSmem s_warp[NW];
+    pdl_enter();
+    const int wib = threadIdx.x >> 5;
+    int member = 0;
+    for (int it = blockIdx.x; it < p.n_items; it += gridDim.x) {
+        while (it >= p.cta_begin[member + 1]) ++member;
+        const MemberDev& md = p.m[member];
+        const int slot = it - p.cta_begin[member];
+        const Control* c = md.ctl;
+        if (*((volatile const int*)&c->done)) continue;  // uniform for the CTA
+        const StepScalars s = c->s;
+        const int snap = c->snap;
+        const double dtd = c->dt;
+        const int gw = slot * NW + wib;
+        const int strip = gw % md.nstrips;
+        const int chunk = gw / md.nstrips;
+        const int r0 = chunk * md.rows_per_warp;
+        const int r1 = min(r0 + md.rows_per_warp, md.d.rows);
+        const int par = p.parity;
+        const StateView in{md.buf[par][0], md.buf[par][1], md.buf[par][2], md.pitch};
+        const StateOut out{md.buf[par ^ 1][0], md.buf[par ^ 1][1], md.buf[par ^ 1][2], md.pitch};
+        StepAccum acc;
+        acc.zero();
+        if (r0 < md.d.rows)
+            march_pair<M, true, MASKED>(md.d, in, out, s, snap, dtd, md.ctl, r0, r1, strip * kWarp * 2,
+                                        s_warp[wib], acc);
+        Accum a;
+        a.maxinv = acc.maxinv;
+        a.vol = acc.vol;
+        a.rain = acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
+        a.outflow = acc.outflow;
+        a.clip = acc.clip;
+        a.mask = acc.mask;
+        finish_run_step<THREADS>(md.d, md.ctl, md.parts, a, false, slot, md.ncta);
+        __syncthreads();  // the fold's shared scratch is free before the next item
     }
 }
 

@@ -68,6 +68,9 @@ EXPORTS = (
     "swe_comm_create",
     "swe_comm_destroy",
     "swe_strip_advance_nccl",
+    "swe_generate_urban",
+    "swe_generate_gamma_hyetograph",
+    "swe_generate_lognormal_field",
     "swe_last_error",
     "swe_version",
 )
@@ -88,6 +91,20 @@ class DomainDesc(ctypes.Structure):
         ("bed", ctypes.c_void_p), ("manning_n", ctypes.c_void_p),
         ("domain_mask", ctypes.c_void_p), ("rainfall_multiplier", ctypes.c_void_p),
         ("fields_on_host", ctypes.c_int32), ("arithmetic", ctypes.c_int32),
+    ]
+
+
+class UrbanDesc(ctypes.Structure):
+    """Mirror of ``swe_urban_desc``."""
+
+    _fields_ = [
+        ("rows", ctypes.c_int32), ("cols", ctypes.c_int32),
+        ("dx", ctypes.c_double), ("slope", ctypes.c_double), ("coverage", ctypes.c_double),
+        ("min_side", ctypes.c_int32), ("max_side", ctypes.c_int32),
+        ("block_raise_m", ctypes.c_double), ("street_offset_m", ctypes.c_double),
+        ("n_block", ctypes.c_double), ("n_street", ctypes.c_double), ("n_scale", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("n_rects", ctypes.c_int32), ("rects", ctypes.c_void_p),
     ]
 
 
@@ -183,6 +200,11 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_comm_destroy": (ctypes.c_int, [_vp]),
         "swe_strip_advance_nccl": (ctypes.c_int, [_vp, _vp, _i32, _i32, _vp, _vp, _vp, _i64, _i32, _f64,
                                                   ctypes.POINTER(RunResult), _vp]),
+        "swe_generate_urban": (ctypes.c_int, [ctypes.POINTER(UrbanDesc), _vp, _vp, _vp, ctypes.POINTER(_i32), _vp]),
+        "swe_generate_gamma_hyetograph": (ctypes.c_int, [_i32, _f64, _f64, _f64, _f64, ctypes.c_uint64, _vp, _vp,
+                                                         _vp]),
+        "swe_generate_lognormal_field": (ctypes.c_int, [_i32, _i32, _f64, _f64, _i32, ctypes.c_uint64, _vp, _vp,
+                                                        _vp]),
         "swe_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
         "swe_version": (ctypes.c_char_p, []),
     }

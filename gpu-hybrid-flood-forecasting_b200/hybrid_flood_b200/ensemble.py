@@ -31,21 +31,40 @@ from .solver import LEDGER_KEYS, SWEState, _ptr, _stream
 DEFAULT_CACHE = pathlib.Path(os.environ.get("SWE_TUNE_CACHE", pathlib.Path.home() / ".cache" / "swe_b200_tune.json"))
 
 
+def _on_device(member: dict) -> bool:
+    fields = [member["bed"], member["manning_n"], member["domain_mask"]]
+    if member.get("rainfall_multiplier") is not None:
+        fields.append(member["rainfall_multiplier"])
+    return all(isinstance(a, torch.Tensor) and a.is_cuda for a in fields)
+
+
 def _desc(member: dict, arithmetic: str, keep: list) -> _lib.DomainDesc:
-    """A ``swe_domain_desc`` for one member (keyword arguments of B200ShallowWaterSolver)."""
+    """A ``swe_domain_desc`` for one member (keyword arguments of B200ShallowWaterSolver).
+
+    Members whose fields are device tensors (``hybrid_flood_b200.generators``)
+    are packed from device memory; others from host arrays."""
     f32 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float32))  # noqa: E731
-    bed = f32(member["bed"])
-    shape = bed.shape
-    man = f32(member["manning_n"])
-    mask = np.ascontiguousarray(np.asarray(member["domain_mask"], dtype=bool).astype(np.uint8))
-    if man.shape != shape or mask.shape != shape:
+    on_dev = _on_device(member)
+    if on_dev:
+        bed = member["bed"].detach().to(torch.float32).contiguous()
+        man = member["manning_n"].detach().to(torch.float32).contiguous()
+        mask = member["domain_mask"].detach().to(torch.uint8).contiguous()
+        ptr = lambda t: t.data_ptr()  # noqa: E731
+    else:
+        bed = f32(member["bed"])
+        man = f32(member["manning_n"])
+        mask = np.ascontiguousarray(np.asarray(member["domain_mask"], dtype=bool).astype(np.uint8))
+        ptr = lambda a: a.ctypes.data  # noqa: E731
+    shape = tuple(bed.shape)
+    if tuple(man.shape) != shape or tuple(mask.shape) != shape:
         raise ValueError("Bed, roughness, and domain mask must have identical shapes.")
     rt = f32(member["rainfall_times_s"]).reshape(-1)
     rr = f32(member["rainfall_rates_m_s"]).reshape(-1)
     if rt.size < 1 or rt.size != rr.size:
         raise ValueError("Rainfall times and rates must be non-empty and of equal length.")
     mult = member.get("rainfall_multiplier")
-    mult = f32(mult) if mult is not None else None
+    if mult is not None:
+        mult = mult.detach().to(torch.float32).contiguous() if on_dev else f32(mult)
     keep.extend([bed, man, mask, rt, rr, mult])
     d = _lib.DomainDesc()
     d.rows, d.cols = shape
@@ -58,9 +77,9 @@ def _desc(member: dict, arithmetic: str, keep: list) -> _lib.DomainDesc:
     d.boundary[:] = list(codes(member.get("boundary", member.get("boundaries"))))
     d.n_rain = rt.size
     d.rain_times, d.rain_rates = rt.ctypes.data, rr.ctypes.data
-    d.bed, d.manning_n, d.domain_mask = bed.ctypes.data, man.ctypes.data, mask.ctypes.data
-    d.rainfall_multiplier = mult.ctypes.data if mult is not None else None
-    d.fields_on_host = 1
+    d.bed, d.manning_n, d.domain_mask = ptr(bed), ptr(man), ptr(mask)
+    d.rainfall_multiplier = ptr(mult) if mult is not None else None
+    d.fields_on_host = 0 if on_dev else 1
     d.arithmetic = _lib.SWE_ARITH_FAST if arithmetic == "fast" else _lib.SWE_ARITH_EXACT
     return d
 
@@ -84,12 +103,13 @@ class B200Ensemble:
             _lib.check(self._lib.swe_ensemble_create(descs, len(members), ctypes.byref(handle)),
                        "swe_ensemble_create")
         self._handle = handle
-        self.shapes = [tuple(np.asarray(m["bed"]).shape) for m in members]
-        self.masks = [torch.from_numpy(np.asarray(m["domain_mask"], dtype=bool)).to(self.device) for m in members]
+        self.shapes = [tuple(m["bed"].shape) for m in members]
+        self.masks = [torch.as_tensor(m["domain_mask"]).to(device=self.device, dtype=torch.bool) for m in members]
         self.arithmetic = arithmetic
         self.rows_per_warp = 64
         self.dry_tolerances = [float(m.get("dry_tolerance_m", 1.0e-4)) for m in members]
-        self.beds = [np.asarray(m["bed"], dtype=np.float32) for m in members]
+        self.beds = [m["bed"].detach().cpu().numpy().astype(np.float32) if isinstance(m["bed"], torch.Tensor)
+                     else np.asarray(m["bed"], dtype=np.float32) for m in members]
 
     def __del__(self):
         h = getattr(self, "_handle", None)

@@ -157,20 +157,32 @@ class B200ShallowWaterSolver:
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
-        to_np = lambda a, dt: (a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)).astype(dt)  # noqa: E731
-        bed_h = np.ascontiguousarray(to_np(bed, np.float32))
-        shape = bed_h.shape
-        man_h = np.ascontiguousarray(to_np(manning_n, np.float32))
-        mask_h = np.ascontiguousarray(to_np(domain_mask, bool))
-        if man_h.shape != shape or mask_h.shape != shape:
+        # Fields already in this device's memory (e.g. from hybrid_flood_b200.generators)
+        # are packed from there; anything else goes through the host.
+        on_dev = all(isinstance(a, torch.Tensor) and a.is_cuda and a.device == self.device
+                     for a in (bed, manning_n, domain_mask)) and (
+            rainfall_multiplier is None or (isinstance(rainfall_multiplier, torch.Tensor)
+                                            and rainfall_multiplier.device == self.device))
+        if on_dev:
+            bed_h = bed.detach().to(torch.float32).contiguous()
+            man_h = manning_n.detach().to(torch.float32).contiguous()
+            mask_h = domain_mask.detach().to(torch.bool).contiguous()
+            mult_h = (rainfall_multiplier.detach().to(torch.float32).contiguous()
+                      if rainfall_multiplier is not None else None)
+        else:
+            to_np = lambda a, dt: (a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)).astype(dt)  # noqa: E731
+            bed_h = np.ascontiguousarray(to_np(bed, np.float32))
+            man_h = np.ascontiguousarray(to_np(manning_n, np.float32))
+            mask_h = np.ascontiguousarray(to_np(domain_mask, bool))
+            mult_h = (np.ascontiguousarray(to_np(rainfall_multiplier, np.float32))
+                      if rainfall_multiplier is not None else None)
+        shape = tuple(bed_h.shape)
+        if tuple(man_h.shape) != shape or tuple(mask_h.shape) != shape:
             raise ValueError("Bed, roughness, and domain mask must have identical shapes.")
-        if bed_h.ndim != 2:
+        if len(shape) != 2:
             raise ValueError("Fields must be two-dimensional [rows, cols].")
-        mult_h = None
-        if rainfall_multiplier is not None:
-            mult_h = np.ascontiguousarray(to_np(rainfall_multiplier, np.float32))
-            if mult_h.shape != shape:
-                raise ValueError("Rainfall multiplier must match the structured-grid shape.")
+        if mult_h is not None and tuple(mult_h.shape) != shape:
+            raise ValueError("Rainfall multiplier must match the structured-grid shape.")
         rt = np.ascontiguousarray(np.asarray(rainfall_times_s, dtype=np.float32).reshape(-1))
         rr = np.ascontiguousarray(np.asarray(rainfall_rates_m_s, dtype=np.float32).reshape(-1))
         if rt.size < 1 or rt.size != rr.size:
@@ -178,7 +190,12 @@ class B200ShallowWaterSolver:
         bnd = codes(boundary if boundary is not None else boundaries)
         if arithmetic not in ("exact", "fast"):
             raise ValueError("arithmetic must be 'exact' or 'fast'")
-        mask_u8 = mask_h.astype(np.uint8)
+        if on_dev:
+            mask_u8 = mask_h.to(torch.uint8)
+            ptr = lambda t: t.data_ptr()  # noqa: E731
+        else:
+            mask_u8 = mask_h.astype(np.uint8)
+            ptr = lambda a: a.ctypes.data  # noqa: E731
         desc = _lib.DomainDesc()
         desc.rows, desc.cols = shape
         desc.dx = desc.dy = float(resolution_m)
@@ -191,11 +208,11 @@ class B200ShallowWaterSolver:
         desc.n_rain = rt.size
         desc.rain_times = rt.ctypes.data
         desc.rain_rates = rr.ctypes.data
-        desc.bed = bed_h.ctypes.data
-        desc.manning_n = man_h.ctypes.data
-        desc.domain_mask = mask_u8.ctypes.data
-        desc.rainfall_multiplier = mult_h.ctypes.data if mult_h is not None else None
-        desc.fields_on_host = 1
+        desc.bed = ptr(bed_h)
+        desc.manning_n = ptr(man_h)
+        desc.domain_mask = ptr(mask_u8)
+        desc.rainfall_multiplier = ptr(mult_h) if mult_h is not None else None
+        desc.fields_on_host = 0 if on_dev else 1
         desc.arithmetic = _lib.SWE_ARITH_FAST if arithmetic == "fast" else _lib.SWE_ARITH_EXACT
         handle = ctypes.c_void_p()
         with torch.cuda.device(self.device):
@@ -208,9 +225,15 @@ class B200ShallowWaterSolver:
             max_dt=float(max_dt_s), default_rainfall_m_s=float(default_rainfall_m_s), boundary=bnd,
             arithmetic=arithmetic, device=self.device,
         )
-        self.domain_mask = torch.from_numpy(mask_h).to(self.device)
-        self.bed = bed_h  # host copy (the output schema's elevation)
+        self.domain_mask = mask_h if on_dev else torch.from_numpy(mask_h).to(self.device)
+        self._bed = bed_h  # the output schema's elevation (host array or device tensor)
         self.shape = tuple(shape)
+
+    @property
+    def bed(self) -> np.ndarray:
+        """Bed elevation as a host float32 array."""
+        b = self._bed
+        return b.cpu().numpy() if isinstance(b, torch.Tensor) else b
 
     def __del__(self):
         h = getattr(self, "_handle", None)

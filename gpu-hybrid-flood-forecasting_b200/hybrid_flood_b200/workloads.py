@@ -125,8 +125,11 @@ def gamma_hyetograph(seed: int, *, values: int = 181, step_s: float = 60.0,
 
 
 def urban_blocks(rows: int, cols: int, rng, *, coverage: float = 0.30,
-                 min_side: int = 5, max_side: int = 20) -> np.ndarray:
-    """Boolean block mask: seeded rectangles until ``coverage`` of the cells is covered."""
+                 min_side: int = 5, max_side: int = 20, rects: list | None = None) -> np.ndarray:
+    """Boolean block mask: seeded rectangles until ``coverage`` of the cells is covered.
+
+    ``rects``, when given, receives the rectangles drawn, in order, as
+    ``(row0, col0, height, width)``."""
     blocks = np.zeros((rows, cols), dtype=bool)
     target = coverage * rows * cols
     covered = 0
@@ -135,10 +138,19 @@ def urban_blocks(rows: int, cols: int, rng, *, coverage: float = 0.30,
         w = int(rng.integers(min_side, max_side + 1))
         r0 = int(rng.integers(0, max(rows - h, 0) + 1))
         c0 = int(rng.integers(0, max(cols - w, 0) + 1))
+        if rects is not None:
+            rects.append((r0, c0, h, w))
         patch = blocks[r0:r0 + h, c0:c0 + w]
         covered += int(patch.size - patch.sum())
         patch[...] = True
     return blocks
+
+
+def urban_rects(rows: int, cols: int, *, seed: int = 1, **kw) -> list:
+    """The rectangles ``urban(rows, cols, seed=seed)`` draws, in order."""
+    rects: list = []
+    urban_blocks(rows, cols, np.random.default_rng(seed), rects=rects, **kw)
+    return rects
 
 
 def urban(rows: int = 2048, cols: int = 2048, *, dx: float = 1.0, seed: int = 1,

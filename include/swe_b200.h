@@ -337,6 +337,52 @@ int swe_strip_advance_nccl(swe_domain_t d, swe_comm_t comm, int32_t rank_below, 
                            float *hu, float *hv, int64_t pitch, int32_t n_steps, double t0,
                            swe_run_result *result, void *stream);
 
+/* ---- Device generators of the synthetic inputs ------------------------------
+ * The reference conditions its terrain on the host from GIS inputs
+ * (src/hybrid_flood/dem/synthetic_terrain.py:114 generate_base_terrain,
+ * src/hybrid_flood/dem/urban_conditioning.py:128 condition_urban_terrain); the
+ * measurement workloads are seeded synthetic fields of the same kind, built
+ * here directly in device memory.  Random draws come from a counter-based
+ * generator (Philox-4x32-10), so a field depends only on its seed and sizes.
+ * Outputs are caller-owned DEVICE buffers; the calls allocate their own
+ * scratch and synchronise the stream before returning. */
+typedef struct {
+    int32_t rows, cols;
+    double dx;                 /* cell size (m) */
+    double slope;              /* plane falling toward +x: slope * (cols*dx - x), x at cell centres */
+    double coverage;           /* block fraction to reach (0.30) */
+    int32_t min_side, max_side;/* block side range in cells (5, 20) */
+    double block_raise_m;      /* +10 m on blocks */
+    double street_offset_m;    /* -0.2 m on streets */
+    double n_block, n_street;  /* Manning n on blocks / streets (0.05, 0.015) */
+    double n_scale;            /* multiplies both */
+    uint64_t seed;
+    int32_t n_rects;           /* > 0: use these rectangles in order instead of drawing them */
+    const int32_t *rects;      /* HOST int32[n_rects][4]: row0, col0, height, width */
+} swe_urban_desc;
+
+/* Urban DEM: rectangles are added in order until the covered cells reach
+ * coverage * rows * cols (a cell covered by several counts once); bed =
+ * float32(plane + raise on blocks, + street offset elsewhere) and manning_n =
+ * float32(n * n_scale), both formed in float64.  block_mask (uint8, may be
+ * NULL) receives 1 on blocks; *blocks_used (may be NULL) the rectangles used. */
+int swe_generate_urban(const swe_urban_desc *q, float *bed, float *manning_n, uint8_t *block_mask,
+                       int32_t *blocks_used, void *stream);
+
+/* Hyetograph of n values step_s apart: times[i] = i*step_s and rates[i] =
+ * Gamma(shape_k, scale) * to_m_s (e.g. scale in mm/h, to_m_s = 1e-3/3600),
+ * Gamma variates by Marsaglia and Tsang's method, rounded to float32. */
+int swe_generate_gamma_hyetograph(int32_t n, double step_s, double shape_k, double scale, double to_m_s,
+                                  uint64_t seed, float *times, float *rates, void *stream);
+
+/* Smoothed log-normal field (a Manning n field): standard normal noise per
+ * cell (or the caller's DEVICE float64 noise[rows*cols] when non-NULL),
+ * smoothed by a reflect-padded separable Gaussian smooth_cells wide (sigma =
+ * smooth_cells/6, taps normalised), divided by its standard deviation, and
+ * out = float32(median * exp(sigma_log * x)). */
+int swe_generate_lognormal_field(int32_t rows, int32_t cols, double median, double sigma_log, int32_t smooth_cells,
+                                 uint64_t seed, const double *noise, float *out, void *stream);
+
 /* Largest cell count swe_max_inverse_dt_noalloc accepts (a 4096 x 4096 grid). */
 #define SWE_NOALLOC_MAX_CELLS 16777216
 

@@ -221,3 +221,59 @@ def test_rollout_backward_matches_stepwise_reverse(cuda_device):
         assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(a)
     ga, gb = gn2_a.cpu().numpy().astype(np.float64), gn2_b.cpu().numpy().astype(np.float64)
     assert np.linalg.norm(ga - gb) <= 1e-3 * np.linalg.norm(ga)
+
+
+def test_gauge_loss_gradients_at_the_adjoint_configuration(cuda_device):
+    """The adjoint configuration at full size: 512x512 (dx = 2 m), log-normal
+    Manning n, 16 gauges every 10 steps, 2000 fixed 0.2 s steps, a checkpoint
+    every 50 steps.  Directional derivatives of the gauge MSE in three random
+    directions for the n field and for the initial depth, and the rain-scale
+    derivative, against central differences of the float64 C oracle with a
+    relative step of 1e-3.  The state stays wet (depth >= 0.2 m), away from
+    wet/dry fronts.  Tolerance 5 % relative: a float32 forward and an adjoint on
+    approximate division/square root over 2000 steps."""
+    from hybrid_flood_b200.adjoint import gauge_rollout
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver
+    from hybrid_flood_b200.workloads import adjoint_case
+
+    w, n_truth, n_est, gauges = adjoint_case(512, 512)
+    kw = w.solver_kwargs()
+    depth = np.maximum(1.0 - w.bed, 0.2).astype(np.float32)
+    steps, dt, every, ckpt = 2000, 0.2, 10, 50
+    obs = GL.rollout_gauges(w.bed, n_truth, w.domain_mask, kw, depth, steps, dt, gauges, every)
+    s = B200ShallowWaterSolver(w.bed, n_est, w.domain_mask, **kw, arithmetic="exact")
+    dev = cuda_device
+    n_t = torch.tensor(n_est, device=dev, requires_grad=True)
+    h_t = torch.tensor(depth, device=dev, requires_grad=True)
+    s_t = torch.tensor(1.0, device=dev, requires_grad=True)
+    pred = gauge_rollout(s, n_t, h_t, s_t, n_steps=steps, dt=dt, gauge_index=gauges, obs_every=every,
+                         checkpoint_every=ckpt)
+    loss = torch.mean((pred - torch.tensor(obs, dtype=torch.float32, device=dev)) ** 2)
+    loss.backward()
+    gn, gh, gs = (n_t.grad.cpu().numpy().astype(np.float64), h_t.grad.cpu().numpy().astype(np.float64),
+                  float(s_t.grad))
+
+    def L(nn=n_est.astype(np.float64), h0=depth.astype(np.float64), scale=1.0):
+        return GL.gauge_mse(GL.rollout_gauges(w.bed, nn, w.domain_mask, kw, h0, steps, dt, gauges, every, scale),
+                            obs)
+
+    assert float(loss.detach()) == pytest.approx(L(), rel=1e-2)
+    eps = 1e-3
+    rng = np.random.default_rng(21)
+    rel = []
+    for _ in range(3):
+        v = rng.normal(0.0, 1.0, w.shape)
+        dn = eps * n_est.astype(np.float64) * v  # relative step of the n field
+        fd = (L(nn=n_est + dn) - L(nn=n_est - dn)) / 2.0
+        ad = float((gn * dn).sum())
+        rel.append(abs(ad - fd) / abs(fd))
+        assert ad == pytest.approx(fd, rel=5e-2)
+        dh = eps * depth.astype(np.float64) * rng.normal(0.0, 1.0, w.shape)  # relative step of h0
+        fd = (L(h0=depth + dh) - L(h0=depth - dh)) / 2.0
+        ad = float((gh * dh).sum())
+        rel.append(abs(ad - fd) / abs(fd))
+        assert ad == pytest.approx(fd, rel=5e-2)
+    fd = (L(scale=1.0 + eps) - L(scale=1.0 - eps)) / (2.0 * eps)
+    rel.append(abs(gs - fd) / abs(fd))
+    assert gs == pytest.approx(fd, rel=5e-2)
+    print(f"config-2 directional derivatives: max relative difference {max(rel):.3g}")
