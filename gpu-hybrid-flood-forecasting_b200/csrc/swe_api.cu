@@ -1136,7 +1136,9 @@ int adjoint_step_impl(swe_domain* d, const float* h, const float* hu, const floa
         adj_cell_kernel<kThreads, true><<<blocks, kThreads, 0, st>>>(al);
     else
         adj_cell_kernel<kThreads, false><<<blocks, kThreads, 0, st>>>(al);
-    adj_face_kernel<kThreads><<<blocks, kThreads, 0, st>>>(al);
+    const int64_t tiles = (int64_t)((d->dd.cols + kAdjTW - 1) / kAdjTW) * ((rows + kAdjTH - 1) / kAdjTH);
+    adj_face_tile_kernel<<<(int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)d->sms * 8)),
+                           kAdjTW * kAdjTH, 0, st>>>(al);
     SWE_CK(cudaGetLastError());
     return SWE_OK;
 }
