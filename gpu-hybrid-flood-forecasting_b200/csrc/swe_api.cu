@@ -122,6 +122,11 @@ struct swe_domain {
     double* corr_sums = nullptr;    // volume sums of the residual correction
     float* corr_prov = nullptr;     // provisional-depth plane of the correction
     unsigned* done_counter = nullptr;  // set by an ensemble: shared completion counter
+    // swe_run_host: device staging of the recorded outputs and the copy stream.
+    float* snap_dev = nullptr;
+    int64_t snap_cap = 0;  // floats
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t snap_ev = nullptr;
     // CUDA graph of kChunk run-mode steps starting from ping buffer 0, and the
     // inputs it was captured with (a change of any of them re-captures it).
     cudaStream_t cap_stream = nullptr;
@@ -523,6 +528,9 @@ void free_domain(swe_domain* d) {
     }
     if (d->chunk_graph) cudaGraphExecDestroy(d->chunk_graph);
     if (d->cap_stream) cudaStreamDestroy(d->cap_stream);
+    cudaFree(d->snap_dev);
+    if (d->copy_stream) cudaStreamDestroy(d->copy_stream);
+    if (d->snap_ev) cudaEventDestroy(d->snap_ev);
     delete d;
 }
 
@@ -1262,6 +1270,113 @@ int swe_run(swe_domain_t d, const float* h0, const float* hu0, const float* hv0,
     }
     if (result->status == SWE_ERR_NONFINITE)
         return fail(SWE_ERR_NONFINITE, "non-finite values reached the CFL reduction");
+    return SWE_OK;
+}
+
+int swe_run_host(swe_domain_t d, const float* h0, const float* hu0, const float* hv0, int64_t pitch_in,
+                 const float* output_times, int32_t n_out, int32_t max_steps, float* out_h, float* out_hu,
+                 float* out_hv, swe_run_result* result, void* stream) {
+    if (!d || !result) return fail(SWE_ERR_INVALID, "null argument");
+    int rc = check_state_ptrs(h0, hu0, hv0, pitch_in, d->dd.cols);
+    if (rc) return rc;
+    if (!output_times || n_out < 1 || output_times[0] != 0.0f)
+        return fail(SWE_ERR_INVALID, "Output times must be one-dimensional, start at zero, and increase.");
+    for (int i = 1; i < n_out; ++i)
+        if (!(output_times[i] > output_times[i - 1]))
+            return fail(SWE_ERR_INVALID, "Output times must be one-dimensional, start at zero, and increase.");
+    if (max_steps < 0) return fail(SWE_ERR_INVALID, "max_steps must be >= 0");
+    if (!out_h || !out_hu || !out_hv) return fail(SWE_ERR_INVALID, "output buffers are required");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int rows = d->dd.rows, cols = d->dd.cols;
+    const int64_t plane = (int64_t)rows * cols;
+    rc = ensure_ping(d);
+    if (rc) return rc;
+    const Plan pl = make_plan(d, d->run_vec, true);
+    rc = ensure_parts(d, std::max(pl.blocks, reduce_blocks(d)));
+    if (rc) return rc;
+    // Device staging: the initial state in ping buffer 1 and one plane triple per output.
+    const int64_t need = (int64_t)n_out * 3 * plane;
+    if (need > d->snap_cap) {
+        cudaFree(d->snap_dev);
+        d->snap_dev = nullptr;
+        d->snap_cap = 0;
+        SWE_CK(cudaMalloc(&d->snap_dev, sizeof(float) * (size_t)need));
+        d->snap_cap = need;
+    }
+    if (!d->copy_stream) SWE_CK(cudaStreamCreateWithFlags(&d->copy_stream, cudaStreamNonBlocking));
+    if (!d->snap_ev) SWE_CK(cudaEventCreateWithFlags(&d->snap_ev, cudaEventDisableTiming));
+    const float* hin[3] = {h0, hu0, hv0};
+    for (int f = 0; f < 3; ++f)
+        SWE_CK(cudaMemcpy2DAsync(d->ping[1][f], sizeof(float) * d->ppitch, hin[f], sizeof(float) * pitch_in,
+                                 sizeof(float) * cols, rows, cudaMemcpyHostToDevice, st));
+    float* sh = d->snap_dev;
+    float* shu = sh + (int64_t)n_out * plane;
+    float* shv = shu + (int64_t)n_out * plane;
+    rc = begin_run(d, StateView{d->ping[1][0], d->ping[1][1], d->ping[1][2], d->ppitch}, output_times, n_out,
+                   (double)output_times[0], n_out, max_steps, sh, shu, shv, st);
+    if (rc) return rc;
+    float* host[3] = {out_h, out_hu, out_hv};
+    float* dev[3] = {sh, shu, shv};
+    int copied = 0;
+    // Copies output k to the host on the copy stream once `ev` (recorded after it was written) has passed.
+    auto copy_out = [&](int upto, cudaEvent_t ev) -> int {
+        if (upto <= copied) return SWE_OK;
+        SWE_CK(cudaStreamWaitEvent(d->copy_stream, ev, 0));
+        for (int f = 0; f < 3; ++f)
+            SWE_CK(cudaMemcpyAsync(host[f] + (int64_t)copied * plane, dev[f] + (int64_t)copied * plane,
+                                   sizeof(float) * (size_t)(upto - copied) * plane, cudaMemcpyDeviceToHost,
+                                   d->copy_stream));
+        copied = upto;
+        return SWE_OK;
+    };
+    SWE_CK(cudaEventRecord(d->snap_ev, st));
+    rc = copy_out(1, d->snap_ev);  // output 0 is the initial state
+    if (rc) return rc;
+    d->launches = 1;
+    d->timed_valid = false;
+    int64_t launched = 0;
+    int chunk = 0;
+    for (;;) {
+        const int64_t todo = std::min<int64_t>(kChunk, (int64_t)max_steps - launched);
+        rc = enqueue_run_steps(d, launched, todo, st);
+        if (rc) return rc;
+        launched += todo;
+        d->launches += todo;
+        const int slot = chunk & 1;
+        SWE_CK(cudaMemcpyAsync(&d->ctl_host[slot], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+        SWE_CK(cudaEventRecord(d->poll_ev[slot], st));
+        if (launched >= max_steps) break;
+        if (chunk > 0) {
+            // The previous chunk has finished: outputs it recorded go to the host
+            // while the chunk just queued runs.
+            SWE_CK(cudaEventSynchronize(d->poll_ev[slot ^ 1]));
+            const Control& c = d->ctl_host[slot ^ 1];
+            rc = copy_out(std::min(c.idx, n_out), d->poll_ev[slot ^ 1]);
+            if (rc) return rc;
+            if (c.done) break;
+        }
+        ++chunk;
+    }
+    SWE_CK(cudaStreamSynchronize(st));
+    SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
+    const Control& c = d->ctl_host[0];
+    SWE_CK(cudaEventRecord(d->snap_ev, st));
+    rc = copy_out(std::min(c.idx, n_out), d->snap_ev);
+    if (rc) return rc;
+    SWE_CK(cudaStreamSynchronize(d->copy_stream));
+    result->final_time_s = c.t;
+    result->outputs_written = c.idx;
+    result->steps_used = c.steps;
+    result->status = c.status ? c.status : (c.idx >= n_out ? SWE_OK : SWE_ERR_MAX_STEPS);
+    result->reserved = 0;
+    for (int i = 0; i < 6; ++i) result->ledger[i] = c.ledger[i];
+    if (result->status == SWE_ERR_MAX_STEPS) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "max_steps=%d wrote %d/%d outputs; last time=%.3f s.", max_steps,
+                      result->outputs_written, n_out, result->final_time_s);
+        return fail(SWE_ERR_MAX_STEPS, msg);
+    }
+    if (result->status == SWE_ERR_NONFINITE) return fail(SWE_ERR_NONFINITE, "non-finite values reached the CFL reduction");
     return SWE_OK;
 }
 

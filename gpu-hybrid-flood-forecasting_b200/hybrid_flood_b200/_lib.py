@@ -33,6 +33,7 @@ EXPORTS = (
     "swe_cfl_dt",
     "swe_rainfall_rate",
     "swe_run",
+    "swe_run_host",
     "swe_advance",
     "swe_last_launch_count",
     "swe_resident_load",
@@ -153,6 +154,8 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_rainfall_rate": (ctypes.c_int, [_vp, _f64, ctypes.POINTER(_f64)]),
         "swe_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _vp, _i32, _i32, _vp, _vp, _vp,
                                    ctypes.POINTER(RunResult), _vp]),
+        "swe_run_host": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _vp, _i32, _i32, _vp, _vp, _vp,
+                                        ctypes.POINTER(RunResult), _vp]),
         "swe_advance": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _i32, _f64,
                                        ctypes.POINTER(RunResult), _vp]),
         "swe_last_launch_count": (ctypes.c_int64, [_vp]),

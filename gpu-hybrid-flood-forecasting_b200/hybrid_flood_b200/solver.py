@@ -276,6 +276,42 @@ class B200ShallowWaterSolver:
             int(res.steps_used), dict(zip(LEDGER_KEYS, list(res.ledger))),
         )
 
+    def run_to_host(self, initial_state, output_times_s, *, max_steps: int = 20_000, out=None) -> RunResult:
+        """``run`` from and to host memory: the reference's NumPy-in, NumPy-out call.
+
+        ``initial_state``: three host arrays ``[rows, cols]`` (NumPy or CPU
+        tensors).  The outputs come back as NumPy arrays ``[n_out, rows, cols]``;
+        each is copied to the host as soon as it is recorded, while the run
+        continues.  ``out``: three preallocated CPU float32 tensors of that
+        shape (pinned memory overlaps the copies); by default pinned ones are
+        allocated.
+        """
+        times = np.asarray(output_times_s, dtype=np.float32)
+        if times.ndim != 1 or not len(times) or times[0] != 0 or np.any(np.diff(times) <= 0):
+            raise ValueError(_OUTPUT_TIMES_MSG)
+        times = np.ascontiguousarray(times)
+        n = len(times)
+        host = []
+        for a in initial_state:
+            t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32))
+            if t.is_cuda or t.dtype != torch.float32 or tuple(t.shape) != self.shape or t.stride(-1) != 1:
+                raise ValueError(f"run_to_host needs host float32 arrays of shape {self.shape}")
+            host.append(t)
+        if out is None:
+            out = [torch.empty((n, *self.shape), dtype=torch.float32).pin_memory() for _ in range(3)]
+        for t in out:
+            if t.is_cuda or t.dtype != torch.float32 or tuple(t.shape) != (n, *self.shape) or not t.is_contiguous():
+                raise ValueError("out must be three contiguous host float32 tensors [n_out, rows, cols]")
+        res = _lib.RunResult()
+        with torch.cuda.device(self.device):
+            rc = self._lib.swe_run_host(
+                self._handle, *(ctypes.c_void_p(t.data_ptr()) for t in host), int(host[0].stride(0)),
+                times.ctypes.data, n, int(max_steps), *(ctypes.c_void_p(t.data_ptr()) for t in out),
+                ctypes.byref(res), _stream(self.device))
+        _lib.check(rc, "run_to_host")
+        return RunResult(SWEState(*(t.numpy() for t in out)), times, float(res.final_time_s),
+                         int(res.outputs_written), int(res.steps_used), dict(zip(LEDGER_KEYS, list(res.ledger))))
+
     def step(self, state, dt: float, time_s: float) -> SWEState:
         return finite_volume_step(state, self.params, dt, time_s)
 

@@ -123,6 +123,16 @@ int swe_run(swe_domain_t d, const float *h0, const float *hu0, const float *hv0,
             int64_t pitch_in, const float *output_times, int32_t n_out, int32_t max_steps,
             float *out_h, float *out_hu, float *out_hv, swe_run_result *result, void *stream);
 
+/* swe_run with the initial state and the outputs in HOST memory: the state is
+ * copied in, and each output is copied back to out_* (HOST float32
+ * [n_out][rows][cols]) as soon as the run has recorded it, on a second stream
+ * while the later steps run.  Page-locked (pinned) host buffers let the copies
+ * overlap the steps; pageable ones work but serialise them.  Same results,
+ * validation and status codes as swe_run. */
+int swe_run_host(swe_domain_t d, const float *h0, const float *hu0, const float *hv0, int64_t pitch_in,
+                 const float *output_times, int32_t n_out, int32_t max_steps, float *out_h, float *out_hu,
+                 float *out_hv, swe_run_result *result, void *stream);
+
 /* Advance (h, hu, hv) in place by exactly n_steps CFL-limited steps starting at
  * time start_s; the state, final time and ledger are returned in `result`. */
 int swe_advance(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, int32_t n_steps,

@@ -79,3 +79,25 @@ def test_run_with_graph_chunks_matches_the_oracle_step_count(cuda_device):
     assert got.steps_used == want[2] and got.steps_used > 64
     for k in range(len(times)):
         assert rel_l2(got.states.h[k].cpu().numpy(), want[0][k, 0]) < 1e-5
+
+
+def test_run_to_host_equals_run(cuda_device):
+    """The host-memory run (outputs copied back while the run continues) gives
+    the same outputs, clock, step count and ledger as the device run."""
+    import numpy as np
+
+    s, init = _case("fast")
+    host = [t.cpu().numpy() for t in init]
+    times = np.asarray([0.0, 5.0, 11.0, 30.0, 31.5], np.float32)
+    a = s.run(init, times)
+    b = s.run_to_host(host, times)
+    assert (a.steps_used, a.outputs_written, a.final_time_s, a.ledger) == (
+        b.steps_used, b.outputs_written, b.final_time_s, b.ledger)
+    for x, y in zip(a.states, b.states):
+        np.testing.assert_array_equal(x.cpu().numpy(), y)
+    out = [torch.zeros((len(times), *s.shape)) for _ in range(3)]  # pageable buffers work too
+    c = s.run_to_host(host, times, out=out)
+    for x, y in zip(a.states, c.states):
+        np.testing.assert_array_equal(x.cpu().numpy(), y)
+    with pytest.raises(RuntimeError, match="max_steps"):
+        s.run_to_host(host, times, max_steps=3)
