@@ -113,6 +113,17 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _tensor_peak():
+    """Dense bf16 TFLOP/s: the sustained cuBLAS figure of MEASURED_PEAKS.json, else the fallback."""
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        for key in ("bf16_tflops_sustained", "bf16_tflops"):
+            if key in d:
+                return float(d[key]), f"measured ({key})"
+    return 1400.0, "fallback (sustained)"
+
+
 class ClockSampler:
     """SM clock and clock-event (throttle) reasons sampled through NVML in a
     background thread every ~0.5 ms; :meth:`summary` keeps the samples taken
@@ -506,6 +517,13 @@ def _hybrid(args, dev):
         e1.record(stream)
     torch.cuda.synchronize(dev)
     net_ms = e0.elapsed_time(e1) / 3
+    # FLOPs of one corrector forward (convolutions and transposed convolutions, 2 per MAC)
+    from torch.utils.flop_counter import FlopCounterMode
+
+    with torch.no_grad(), FlopCounterMode(display=False) as fc:
+        net(feats)
+    net_flops = float(fc.get_total_flops())
+    tf_peak, tf_kind = _tensor_peak()
     cells = M * S * S
     phys_updates = float(S * S * steps.sum())
     finite = all(bool(torch.isfinite(t).all()) for tr in traj for t in tr)
@@ -515,6 +533,10 @@ def _hybrid(args, dev):
             "ms_per_interval": total_ms / args.hybrid_intervals, "physics_steps_mean": float(steps.mean()),
             "physics_steps_max": int(steps.max()), "corrector_ms_per_interval": net_ms,
             "corrector_share": net_ms * args.hybrid_intervals / total_ms,
+            "corrector_tflop_per_forward": net_flops / 1e12,
+            "corrector_tflops": net_flops / (net_ms / 1e3) / 1e12,
+            "corrector_frac_of_bf16_peak": net_flops / (net_ms / 1e3) / 1e12 / tf_peak,
+            "bf16_peak_tflops": tf_peak, "bf16_peak_kind": tf_kind,
             "physics_ms_per_interval": tm.get("physics_ms", 0.0) / args.hybrid_intervals,
             "physics_cell_updates_per_s": phys_updates / (tm["physics_ms"] / 1e3) if tm.get("physics_ms") else None,
             "cell_updates_per_s": phys_updates / (total_ms / 1e3), "finite": finite}
