@@ -179,6 +179,24 @@ class ClockSampler:
     def mark_start(self):
         self.window = (time.perf_counter(), None)
 
+    def sample_until(self, event, min_samples: int = 3):
+        """Sample on this thread while `event` (the end of the timed region) has
+        not completed: a short region (a few launches) still gets samples taken
+        while its kernels run."""
+        if self._nv is None:
+            return
+        nv = self._nv
+        taken = 0
+        while taken < 1000 and not event.query():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self._h))
+            except Exception:  # noqa: BLE001
+                return
+            if not event.query():  # keep only samples taken before the region ended
+                self.samples.append((time.perf_counter(), mhz, rs))
+                taken += 1
+
     def mark_end(self):
         self.window = (self.window[0], time.perf_counter())
 
@@ -730,6 +748,7 @@ def run_b200(args, rank: int, world: int):
         start.record(stream)
         solver.resident_steps(args.steps)
         end.record(stream)
+        clocks.sample_until(end)
         torch.cuda.synchronize(dev)
         clocks.mark_end()
     if dist:
