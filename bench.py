@@ -385,7 +385,7 @@ def _ensemble(args, dev, rank: int, world: int):
     states = ens.initial_states(depths)
     ens.advance_(states, 50)  # spin-up
     tune_states = [type(s)(*(t.clone() for t in s)) for s in states]
-    best = ens.autotune(tune_states, candidates=(16, 32, 64, 128), steps=50, cache=None)
+    best = ens.autotune(tune_states, candidates=(32, 64, 128, 256), steps=50, cache=None)
     del tune_states
     ens.advance_(states, 50)  # warm-up (graph capture)
     if world > 1:

@@ -49,12 +49,35 @@ __device__ __forceinline__ float apow(float x, float e) {  // x > 0
     return r;
 }
 
+// One side of a face: the cell's state, its velocities (m/h where h > dry, else
+// 0: computed once per cell and shared by the cell's four faces) and whether it
+// is active.
 struct FaceIn {
-    float h, hu, hv, z;
+    float h, hu, hv, z, u, v;
     bool act;
 };
 
-__device__ __forceinline__ FaceIn face_in(const Cell& c) { return {c.h, c.hu, c.hv, c.z, active(c.nm)}; }
+__device__ __forceinline__ FaceIn face_in(float h, float hu, float hv, float z, bool act, float dry) {
+    const bool wet = h > dry;
+    return {h, hu, hv, z, wet ? adiv(hu, h) : 0.f, wet ? adiv(hv, h) : 0.f, act};
+}
+
+__device__ __forceinline__ FaceIn face_in(const Cell& c, float dry) {
+    return face_in(c.h, c.hu, c.hv, c.z, active(c.nm), dry);
+}
+
+// The mirrored copy of a cell across a wall: the normal momentum and velocity change sign.
+template <int AXIS>
+__device__ __forceinline__ FaceIn mirror(FaceIn c) {
+    if (AXIS == 1) {
+        c.hu = -c.hu;
+        c.u = -c.u;
+    } else {
+        c.hv = -c.hv;
+        c.v = -c.v;
+    }
+    return c;
+}
 
 // Forward flux of one face (plain float32 arithmetic; the adjoint needs the
 // values, not the reference's bit pattern).
@@ -65,16 +88,13 @@ __device__ void adj_face_fwd(FaceIn lo, FaceIn hi, const AdjConsts& k, float F[3
     if (!(lo.act || hi.act)) return;
     FaceIn L = lo, R = hi;
     if (lo.act && !hi.act) {
-        R = lo;
-        if (AXIS == 1) R.hu = -lo.hu; else R.hv = -lo.hv;
+        R = mirror<AXIS>(lo);
     } else if (!lo.act && hi.act) {
-        L = hi;
-        if (AXIS == 1) L.hu = -hi.hu; else L.hv = -hi.hv;
+        L = mirror<AXIS>(hi);
     }
     const float zf = fmaxf(L.z, R.z);
     const float HL = fmaxf(L.h + L.z - zf, 0.f), HR = fmaxf(R.h + R.z - zf, 0.f);
-    const float uL = L.h > k.dry ? adiv(L.hu, L.h) : 0.f, vL = L.h > k.dry ? adiv(L.hv, L.h) : 0.f;
-    const float uR = R.h > k.dry ? adiv(R.hu, R.h) : 0.f, vR = R.h > k.dry ? adiv(R.hv, R.h) : 0.f;
+    const float uL = L.u, vL = L.v, uR = R.u, vR = R.v;
     const float XL = HL * uL, YL = HL * vL, XR = HR * uR, YR = HR * vR;
     const float nL = AXIS == 1 ? XL : YL, nR = AXIS == 1 ? XR : YR;
     const float unL = HL > k.dry ? adiv(nL, HL) : 0.f, unR = HR > k.dry ? adiv(nR, HR) : 0.f;
@@ -112,19 +132,16 @@ __device__ void adj_face_vjp(FaceIn lo, FaceIn hi, const AdjConsts& k, const flo
     const bool hi_wall = lo.act && !hi.act, lo_wall = !lo.act && hi.act;
     FaceIn L = lo, R = hi;
     if (hi_wall) {
-        R = lo;
-        if (AXIS == 1) R.hu = -lo.hu; else R.hv = -lo.hv;
+        R = mirror<AXIS>(lo);
     } else if (lo_wall) {
-        L = hi;
-        if (AXIS == 1) L.hu = -hi.hu; else L.hv = -hi.hv;
+        L = mirror<AXIS>(hi);
     }
     // ---- forward, keeping what the reverse needs ----
     const float zf = fmaxf(L.z, R.z);
     const float aL = L.h + L.z - zf, aR = R.h + R.z - zf;
     const float HL = fmaxf(aL, 0.f), HR = fmaxf(aR, 0.f);
     const bool dL = L.h > k.dry, dR = R.h > k.dry;
-    const float uL = dL ? adiv(L.hu, L.h) : 0.f, vL = dL ? adiv(L.hv, L.h) : 0.f;
-    const float uR = dR ? adiv(R.hu, R.h) : 0.f, vR = dR ? adiv(R.hv, R.h) : 0.f;
+    const float uL = L.u, vL = L.v, uR = R.u, vR = R.v;
     const float XL = HL * uL, YL = HL * vL, XR = HR * uR, YR = HR * vR;
     const float nL = AXIS == 1 ? XL : YL, nR = AXIS == 1 ? XR : YR;
     const bool wL = HL > k.dry, wR = HR > k.dry;
@@ -284,9 +301,10 @@ __device__ __forceinline__ Cell adj_load(const DomainDev& d, const StateView& s,
 // pointwise part.
 __device__ void adj_cell_update(const AdjLaunch& p, int r, int c, float upd[3]) {
     const DomainDev& d = p.d;
-    const FaceIn C = face_in(adj_load(d, p.in, r, c));
-    const FaceIn W = face_in(adj_load(d, p.in, r, c - 1)), E = face_in(adj_load(d, p.in, r, c + 1));
-    const FaceIn S = face_in(adj_load(d, p.in, r - 1, c)), N = face_in(adj_load(d, p.in, r + 1, c));
+    const float dry = p.k.dry;
+    const FaceIn C = face_in(adj_load(d, p.in, r, c), dry);
+    const FaceIn W = face_in(adj_load(d, p.in, r, c - 1), dry), E = face_in(adj_load(d, p.in, r, c + 1), dry);
+    const FaceIn S = face_in(adj_load(d, p.in, r - 1, c), dry), N = face_in(adj_load(d, p.in, r + 1, c), dry);
     float Fl[3], Fr[3], Fb[3], Ft[3], cl_lo, cl_hi, cr_lo, cr_hi, cb_lo, cb_hi, ct_lo, ct_hi;
     adj_face_fwd<1>(W, C, p.k, Fl, cl_lo, cl_hi);
     adj_face_fwd<1>(C, E, p.k, Fr, cr_lo, cr_hi);
@@ -324,55 +342,57 @@ __device__ __forceinline__ bool adj_upd_from_next(const AdjLaunch& p, int r, int
     return true;
 }
 
-template <int THREADS, bool NEXT>
-__global__ void __launch_bounds__(THREADS) adj_cell_kernel(const AdjLaunch p) {
+// Reverse of the pointwise part of cell (r, c) (rain, clip, friction, masks):
+// returns lupd = dL/d(upd) (zero for an inactive cell); when `owned`, also adds
+// the cell's dL/d(n^2) to grad_n2 and its rain-scale term to *rain_acc.
+template <bool NEXT>
+__device__ __forceinline__ void adj_cell_at(const AdjLaunch& p, int r, int c, bool owned, double* rain_acc,
+                                            float lu[3]) {
     const DomainDev& d = p.d;
-    const int64_t n = (int64_t)d.rows * d.cols;
-    double rain_acc = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * THREADS) {
-        const int r = (int)(i / d.cols), c = (int)(i - (int64_t)r * d.cols);
-        const float nm = d.nm[(int64_t)r * d.spitch + c];
-        const bool act = active(nm);
-        const int64_t lo = (int64_t)r * p.lpitch + c;
-        if (!act) {
-            p.lupd[0][lo] = p.lupd[1][lo] = p.lupd[2][lo] = 0.f;
-            continue;
-        }
-        const float mult = d.mult ? d.mult[(int64_t)r * d.spitch + c] : 1.f;
-        float upd[3];
-        // upd[0] below is the depth after the rain (before the clip).
-        if (!(NEXT && adj_upd_from_next(p, r, c, fabsf(nm), upd))) {
-            adj_cell_update(p, r, c, upd);
-            upd[0] += p.s.dt_rain * mult;
-        }
-        const float h = fmaxf(upd[0], 0.f);
-        const float norm = asqrt(upd[1] * upd[1] + upd[2] * upd[2]);
-        const float m = fmaxf(h, p.k.dry);
-        const float pw = apow(m, -7.0f / 3.0f);
-        const float n2 = fabsf(nm);
-        const float fr = p.s.dt_g * n2 * norm * pw;
-        const float den = 1.f + fr;
-        const float rden = adiv(1.f, den);
-        const float qx = upd[1] * rden, qy = upd[2] * rden;
-        const bool wet = h > p.k.dry;
-        const int64_t li = (int64_t)r * p.lam.pitch + c;
-        const float lqx = wet ? p.lam.hu[li] : 0.f, lqy = wet ? p.lam.hv[li] : 0.f;
-        float lh = p.lam.h[li];
-        const float lden = -(lqx * qx + lqy * qy) * rden;
-        float lu1 = lqx * rden, lu2 = lqy * rden;
-        if (norm > 0.f) {
-            const float lnorm = lden * p.s.dt_g * n2 * pw;
-            lu1 += adiv(lnorm * upd[1], norm);
-            lu2 += adiv(lnorm * upd[2], norm);
-        }
-        p.grad_n2[(int64_t)r * d.cols + c] += lden * p.s.dt_g * norm * pw;
-        if (h > p.k.dry) lh += adiv(lden * fr * (-7.0f / 3.0f), h);
-        const float lu0 = upd[0] > 0.f ? lh : 0.f;
-        rain_acc += (double)lu0 * (double)p.dt_rate * (double)mult;
-        p.lupd[0][lo] = lu0;
-        p.lupd[1][lo] = lu1;
-        p.lupd[2][lo] = lu2;
+    const float nm = d.nm[(int64_t)r * d.spitch + c];
+    lu[0] = lu[1] = lu[2] = 0.f;
+    if (!active(nm)) return;
+    const float mult = d.mult ? d.mult[(int64_t)r * d.spitch + c] : 1.f;
+    float upd[3];
+    // upd[0] below is the depth after the rain (before the clip).
+    if (!(NEXT && adj_upd_from_next(p, r, c, fabsf(nm), upd))) {
+        adj_cell_update(p, r, c, upd);
+        upd[0] += p.s.dt_rain * mult;
     }
+    const float h = fmaxf(upd[0], 0.f);
+    const float norm = asqrt(upd[1] * upd[1] + upd[2] * upd[2]);
+    const float m = fmaxf(h, p.k.dry);
+    const float pw = apow(m, -7.0f / 3.0f);
+    const float n2 = fabsf(nm);
+    const float fr = p.s.dt_g * n2 * norm * pw;
+    const float den = 1.f + fr;
+    const float rden = adiv(1.f, den);
+    const float qx = upd[1] * rden, qy = upd[2] * rden;
+    const bool wet = h > p.k.dry;
+    const int64_t li = (int64_t)r * p.lam.pitch + c;
+    const float lqx = wet ? p.lam.hu[li] : 0.f, lqy = wet ? p.lam.hv[li] : 0.f;
+    float lh = p.lam.h[li];
+    const float lden = -(lqx * qx + lqy * qy) * rden;
+    float lu1 = lqx * rden, lu2 = lqy * rden;
+    if (norm > 0.f) {
+        const float lnorm = lden * p.s.dt_g * n2 * pw;
+        lu1 += adiv(lnorm * upd[1], norm);
+        lu2 += adiv(lnorm * upd[2], norm);
+    }
+    if (h > p.k.dry) lh += adiv(lden * fr * (-7.0f / 3.0f), h);
+    const float lu0 = upd[0] > 0.f ? lh : 0.f;
+    if (owned) {
+        p.grad_n2[(int64_t)r * d.cols + c] += lden * p.s.dt_g * norm * pw;
+        *rain_acc += (double)lu0 * (double)p.dt_rate * (double)mult;
+    }
+    lu[0] = lu0;
+    lu[1] = lu1;
+    lu[2] = lu2;
+}
+
+// Adds a CTA's rain-scale gradient to the device scalar (one atomic per CTA).
+template <int THREADS>
+__device__ __forceinline__ void adj_flush_rain(const AdjLaunch& p, double rain_acc) {
     rain_acc = warp_sum(rain_acc);
     __shared__ double s_r[THREADS / kWarp];
     if ((threadIdx.x & 31) == 0) s_r[threadIdx.x >> 5] = rain_acc;
@@ -382,6 +402,23 @@ __global__ void __launch_bounds__(THREADS) adj_cell_kernel(const AdjLaunch p) {
         for (int w = 0; w < THREADS / kWarp; ++w) t += s_r[w];
         if (t != 0.0) atomicAdd(p.grad_rain, t);
     }
+}
+
+template <int THREADS, bool NEXT>
+__global__ void __launch_bounds__(THREADS) adj_cell_kernel(const AdjLaunch p) {
+    const DomainDev& d = p.d;
+    const int64_t n = (int64_t)d.rows * d.cols;
+    double rain_acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * THREADS) {
+        const int r = (int)(i / d.cols), c = (int)(i - (int64_t)r * d.cols);
+        float lu[3];
+        adj_cell_at<NEXT>(p, r, c, true, &rain_acc, lu);
+        const int64_t lo = (int64_t)r * p.lpitch + c;
+        p.lupd[0][lo] = lu[0];
+        p.lupd[1][lo] = lu[1];
+        p.lupd[2][lo] = lu[2];
+    }
+    adj_flush_rain<THREADS>(p, rain_acc);
 }
 
 // dL/d(upd) of cell (r, c); zero outside the grid (ghost cells are not updated).
@@ -402,7 +439,7 @@ __device__ __forceinline__ void lupd_at(const AdjLaunch& p, int r, int c, float 
 template <int AXIS>
 __device__ __forceinline__ void adj_face_at(const AdjLaunch& p, int rl, int cl, int rh, int ch, float a,
                                             float* dlo, float* dhi) {
-    const FaceIn L = face_in(adj_load(p.d, p.in, rl, cl)), H = face_in(adj_load(p.d, p.in, rh, ch));
+    const FaceIn L = face_in(adj_load(p.d, p.in, rl, cl), p.k.dry), H = face_in(adj_load(p.d, p.in, rh, ch), p.k.dry);
     float ll[3], lh[3], lF[3];
     lupd_at(p, rl, cl, ll);
     lupd_at(p, rh, ch, lh);
@@ -483,6 +520,129 @@ __global__ void __launch_bounds__(kAdjTW * kAdjTH) adj_face_tile_kernel(const Ad
         }
         __syncthreads();  // the next tile reuses the shared faces
     }
+}
+
+// The whole reverse step in one kernel, for lam_out not aliasing lam.  A CTA
+// of 256 threads takes a tile of 32 x 16 cells and stages, for the tile and its
+// one-cell halo ring (34 x 18 cells), each cell's state, velocities and
+// dL/d(upd) in shared memory (phase 0: the pointwise reverse of adj_cell_at;
+// halo cells are recomputed, but only the tile's own cells add to the n^2 and
+// rain-scale gradients).  Phase 1 evaluates every face of the tile once
+// (16 x 33 x-faces and 17 x 32 y-faces over the 256 threads) from the staged
+// cells; phase 2 gathers the four faces of each cell.  Reading the halo cells'
+// lam while neighbouring tiles write lam_out is why the two must not alias.
+constexpr int kFTW = 32, kFTH = 16, kFHW = kFTW + 2, kFHH = kFTH + 2, kFThreads = 256;
+
+struct AdjTileSmem {
+    float h[kFHH][kFHW], hu[kFHH][kFHW], hv[kFHH][kFHW], z[kFHH][kFHW], u[kFHH][kFHW], v[kFHH][kFHW];
+    float l[3][kFHH][kFHW];
+    float fx[kFTH][kFTW + 1][6];  // face left of tile column c: dlo (0..2), dhi (3..5)
+    float fy[kFTH + 1][kFTW][6];  // face below tile row r
+    unsigned char act[kFHH][kFHW];
+};
+
+__device__ __forceinline__ FaceIn staged(const AdjTileSmem& S, int hr, int hc) {
+    return {S.h[hr][hc], S.hu[hr][hc], S.hv[hr][hc], S.z[hr][hc], S.u[hr][hc], S.v[hr][hc], S.act[hr][hc] != 0};
+}
+
+template <int AXIS>
+__device__ __forceinline__ void staged_face(const AdjTileSmem& S, const AdjConsts& k, int lr, int lc, int hr, int hc,
+                                            float a, float* out) {
+    constexpr int nq = AXIS == 1 ? 1 : 2;
+    float lF[3], lo[3], hi[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) lF[q] = -a * S.l[q][lr][lc] + a * S.l[q][hr][hc];
+    adj_face_vjp<AXIS>(staged(S, lr, lc), staged(S, hr, hc), k, lF, -a * S.l[nq][lr][lc], a * S.l[nq][hr][hc], lo, hi);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        out[q] = lo[q];
+        out[3 + q] = hi[q];
+    }
+}
+
+template <bool NEXT>
+__global__ void __launch_bounds__(kFThreads) adj_tile_kernel(const AdjLaunch p) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    AdjTileSmem& S = *reinterpret_cast<AdjTileSmem*>(s_raw);
+    const DomainDev& d = p.d;
+    const int tiles_x = (d.cols + kFTW - 1) / kFTW, tiles_y = (d.rows + kFTH - 1) / kFTH;
+    const float ax = p.s.dt * p.rdx, ay = p.s.dt * p.rdy;
+    double rain_acc = 0.0;
+    for (int tile = blockIdx.x; tile < tiles_x * tiles_y; tile += gridDim.x) {
+        const int c0 = (tile % tiles_x) * kFTW, r0 = (tile / tiles_x) * kFTH;
+        // Phase 0: the tile and its halo ring (ghost cells outside the grid carry no dL/d(upd)).
+        for (int i = threadIdx.x; i < kFHH * kFHW; i += kFThreads) {
+            const int hr = i / kFHW, hc = i - hr * kFHW;
+            const int r = r0 - 1 + hr, c = c0 - 1 + hc;
+            const FaceIn f = face_in(adj_load(d, p.in, r, c), p.k.dry);
+            S.h[hr][hc] = f.h;
+            S.hu[hr][hc] = f.hu;
+            S.hv[hr][hc] = f.hv;
+            S.z[hr][hc] = f.z;
+            S.u[hr][hc] = f.u;
+            S.v[hr][hc] = f.v;
+            S.act[hr][hc] = f.act ? 1 : 0;
+            float lu[3] = {0.f, 0.f, 0.f};
+            if (r >= 0 && r < d.rows && c >= 0 && c < d.cols) {
+                const bool owned = hr >= 1 && hr <= kFTH && hc >= 1 && hc <= kFTW;
+                adj_cell_at<NEXT>(p, r, c, owned, &rain_acc, lu);
+            }
+            S.l[0][hr][hc] = lu[0];
+            S.l[1][hr][hc] = lu[1];
+            S.l[2][hr][hc] = lu[2];
+        }
+        __syncthreads();
+        // Phase 1: x-faces exist for rows [0, rows) and columns [0, cols] (left of
+        // column c), y-faces for columns [0, cols) and rows [0, rows] (below row r).
+        constexpr int NX = kFTH * (kFTW + 1), NY = (kFTH + 1) * kFTW;
+        for (int f = threadIdx.x; f < NX + NY; f += kFThreads) {
+            if (f < NX) {
+                const int ty = f / (kFTW + 1), tx = f - ty * (kFTW + 1);
+                if (r0 + ty < d.rows && c0 + tx <= d.cols)
+                    staged_face<1>(S, p.k, ty + 1, tx, ty + 1, tx + 1, ax, S.fx[ty][tx]);
+            } else {
+                const int g = f - NX, ty = g / kFTW, tx = g - ty * kFTW;
+                if (c0 + tx < d.cols && r0 + ty <= d.rows)
+                    staged_face<0>(S, p.k, ty, tx + 1, ty + 1, tx + 1, ay, S.fy[ty][tx]);
+            }
+        }
+        __syncthreads();
+        // Phase 2: each cell of the tile adds its side of its four faces.
+        for (int i = threadIdx.x; i < kFTH * kFTW; i += kFThreads) {
+            const int ty = i / kFTW, tx = i - ty * kFTW;
+            const int r = r0 + ty, c = c0 + tx;
+            if (r >= d.rows || c >= d.cols) continue;
+            const float* fl = S.fx[ty][tx];
+            const float* fr = S.fx[ty][tx + 1];
+            const float* fb = S.fy[ty][tx];
+            const float* ft = S.fy[ty + 1][tx];
+            float g[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) g[q] = S.l[q][ty + 1][tx + 1] + fl[3 + q] + fr[q] + fb[3 + q] + ft[q];
+            if (c == 0) {
+                const float s = d.bnd[0] == 0 ? -1.f : 1.f;
+                g[0] += fl[0]; g[1] += s * fl[1]; g[2] += fl[2];
+            }
+            if (c == d.cols - 1) {
+                const float s = d.bnd[1] == 0 ? -1.f : 1.f;
+                g[0] += fr[3]; g[1] += s * fr[4]; g[2] += fr[5];
+            }
+            if (r == 0) {
+                const float s = d.bnd[2] == 0 ? -1.f : 1.f;
+                g[0] += fb[0]; g[1] += fb[1]; g[2] += s * fb[2];
+            }
+            if (r == d.rows - 1) {
+                const float s = d.bnd[3] == 0 ? -1.f : 1.f;
+                g[0] += ft[3]; g[1] += ft[4]; g[2] += s * ft[5];
+            }
+            const int64_t o = (int64_t)r * p.lam_out.pitch + c;
+            p.lam_out.h[o] = g[0];
+            p.lam_out.hu[o] = g[1];
+            p.lam_out.hv[o] = g[2];
+        }
+        __syncthreads();  // the next tile reuses the shared planes
+    }
+    adj_flush_rain<kFThreads>(p, rain_acc);
 }
 
 }  // namespace swe

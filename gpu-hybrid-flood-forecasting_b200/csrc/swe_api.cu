@@ -563,7 +563,7 @@ struct swe_ensemble {
     std::vector<swe_domain*> doms;
     int arith = SWE_ARITH_FAST;
     bool masked = false;
-    int rows_per_warp = 64;  // best measured on the 64-member mix (16: 62, 32: 79, 64: 82 G cell-updates/s)
+    int rows_per_warp = 128;  // a good default on the 64-member mix; B200Ensemble.autotune searches 32-256
     int sms = 148;
     MemberDev* members_dev = nullptr;
     int members_cap = 0;
@@ -1140,13 +1140,33 @@ int adjoint_step_impl(swe_domain* d, const float* h, const float* hu, const floa
     al.rdy = 1.0f / d->dd.k.dy;
     const int64_t n = (int64_t)rows * d->dd.cols;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + kThreads - 1) / kThreads, (int64_t)d->sms * 16));
-    if (next)
-        adj_cell_kernel<kThreads, true><<<blocks, kThreads, 0, st>>>(al);
-    else
-        adj_cell_kernel<kThreads, false><<<blocks, kThreads, 0, st>>>(al);
-    const int64_t tiles = (int64_t)((d->dd.cols + kAdjTW - 1) / kAdjTW) * ((rows + kAdjTH - 1) / kAdjTH);
-    adj_face_tile_kernel<<<(int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)d->sms * 8)),
-                           kAdjTW * kAdjTH, 0, st>>>(al);
+    const bool aliased = lam_h_out == lam_h || lam_hu_out == lam_hu || lam_hv_out == lam_hv;
+    if (!aliased) {
+        // One fused kernel (its halo reads of lam need lam_out elsewhere).
+        static std::once_flag attr_once[2];
+        std::call_once(attr_once[next ? 1 : 0], [&] {
+            if (next)
+                cudaFuncSetAttribute(adj_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(AdjTileSmem));
+            else
+                cudaFuncSetAttribute(adj_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(AdjTileSmem));
+        });
+        const int64_t tiles = (int64_t)((d->dd.cols + kFTW - 1) / kFTW) * ((rows + kFTH - 1) / kFTH);
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)d->sms * 4));
+        if (next)
+            adj_tile_kernel<true><<<grid, kFThreads, sizeof(AdjTileSmem), st>>>(al);
+        else
+            adj_tile_kernel<false><<<grid, kFThreads, sizeof(AdjTileSmem), st>>>(al);
+    } else {
+        if (next)
+            adj_cell_kernel<kThreads, true><<<blocks, kThreads, 0, st>>>(al);
+        else
+            adj_cell_kernel<kThreads, false><<<blocks, kThreads, 0, st>>>(al);
+        const int64_t tiles = (int64_t)((d->dd.cols + kAdjTW - 1) / kAdjTW) * ((rows + kAdjTH - 1) / kAdjTH);
+        adj_face_tile_kernel<<<(int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)d->sms * 8)),
+                               kAdjTW * kAdjTH, 0, st>>>(al);
+    }
     SWE_CK(cudaGetLastError());
     return SWE_OK;
 }
@@ -1689,7 +1709,13 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
     const int rows = d->dd.rows, cols = d->dd.cols;
     const int64_t plane = (int64_t)rows * cols;
     if (!d->next_scratch) SWE_CK(cudaMalloc(&d->next_scratch, sizeof(float) * 3 * (size_t)plane));
+    if (!d->lupd[0]) {
+        d->lpitch = round_up(d->dd.cols, 128);
+        for (int q = 0; q < 3; ++q) SWE_CK(cudaMalloc(&d->lupd[q], sizeof(float) * (size_t)d->lpitch * rows));
+    }
     float* lam[3] = {lam_h, lam_hu, lam_hv};
+    float* alt[3] = {d->lupd[0], d->lupd[1], d->lupd[2]};  // the other half of the lam ping-pong
+    int cur = 0;  // 0: dL/dU of the current step is in lam, 1: in alt
     if (!lam_in)
         for (int f = 0; f < 3; ++f)
             SWE_CK(cudaMemset2DAsync(lam[f], sizeof(float) * lam_pitch, 0, sizeof(float) * cols, rows, st));
@@ -1717,16 +1743,27 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
             if (rc) return rc;
         }
         for (int k = k1 - 1; k >= k0; --k) {
+            // dL/dU_{k+1} is in buffer `cur`; dL/dU_k goes to the other one (the fused
+            // reverse step reads its neighbours' lam while it writes lam_out).
+            float* const* src = cur ? alt : lam;
+            float* const* dst = cur ? lam : alt;
+            const int64_t sp = cur ? d->lpitch : lam_pitch, dp = cur ? lam_pitch : d->lpitch;
             if (n_gauges > 0 && (k + 1) % obs_every == 0) {
                 gauge_inject_kernel<<<(n_gauges + 127) / 128, 128, 0, st>>>(
-                    lam_h, lam_pitch, cols, gauge_index, n_gauges,
-                    grad_obs + (int64_t)((k + 1) / obs_every - 1) * n_gauges);
+                    src[0], sp, cols, gauge_index, n_gauges, grad_obs + (int64_t)((k + 1) / obs_every - 1) * n_gauges);
             }
             const float* a = seg + (int64_t)(k - k0) * 3 * plane;
             const float* nx = k + 1 < k1 ? seg + (int64_t)(k + 1 - k0) * 3 * plane : d->next_scratch;
-            rc = adjoint_step_impl(d, a, a + plane, a + 2 * plane, cols, nx, cols, plane, lam_h, lam_hu, lam_hv,
-                                   lam_pitch, lam_h, lam_hu, lam_hv, lam_pitch, grad_n2, grad_rain_scale,
-                                   dts ? dts[k] : dt, step_time(k, dt, t0, dts), st);
+            rc = adjoint_step_impl(d, a, a + plane, a + 2 * plane, cols, nx, cols, plane, src[0], src[1], src[2], sp,
+                                   dst[0], dst[1], dst[2], dp, grad_n2, grad_rain_scale, dts ? dts[k] : dt,
+                                   step_time(k, dt, t0, dts), st);
+            if (rc) return rc;
+            cur ^= 1;
+        }
+    }
+    if (cur) {  // the result is in the alternate buffers: copy it to the caller's lam planes
+        for (int f = 0; f < 3; ++f) {
+            rc = copy_plane(lam[f], lam_pitch, alt[f], d->lpitch, rows, cols, st);
             if (rc) return rc;
         }
     }

@@ -106,7 +106,7 @@ class B200Ensemble:
         self.shapes = [tuple(m["bed"].shape) for m in members]
         self.masks = [torch.as_tensor(m["domain_mask"]).to(device=self.device, dtype=torch.bool) for m in members]
         self.arithmetic = arithmetic
-        self.rows_per_warp = 64
+        self.rows_per_warp = 128
         self.dry_tolerances = [float(m.get("dry_tolerance_m", 1.0e-4)) for m in members]
         self.beds = [m["bed"].detach().cpu().numpy().astype(np.float32) if isinstance(m["bed"], torch.Tensor)
                      else np.asarray(m["bed"], dtype=np.float32) for m in members]
@@ -228,7 +228,7 @@ class B200Ensemble:
                            "device": torch.cuda.get_device_name(self.device)})
         return hashlib.sha1(text.encode()).hexdigest()[:16]
 
-    def autotune(self, states: list[SWEState], candidates=(8, 16, 32, 64), steps: int = 20,
+    def autotune(self, states: list[SWEState], candidates=(32, 64, 128, 256), steps: int = 50,
                  cache: pathlib.Path | None = DEFAULT_CACHE) -> int:
         """Pick the rows-per-warp of the work list by timing ``steps`` steps per candidate.
 
