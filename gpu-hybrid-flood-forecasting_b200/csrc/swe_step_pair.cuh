@@ -180,18 +180,6 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
 
     CellT<float2> R0, R1;
     float2 yT0, yT1, yT2;
-    consume(0, R1);  // row r0-1
-    consume(1, R0);  // row r0
-    {
-        const FaceT<float2> f = face_t<0, M, MASKED>(R1, R0, kp);
-        yT0 = f.f0;
-        yT1 = f.f1;
-        yT2 = A::add(f.f2, f.corr_hi);
-        if constexpr (RUN) {
-            if (r0 == 0) lg.out_y = lfma(neg(f.f0), vmask, lg.out_y);
-        }
-    }
-    consume(2, R1);  // row r0+1
 
     // The x-faces of a row: (cell 0 | cell 1) and (cell 1 | first cell of the next lane).
     // Returns the lo-side fluxes of both cells' left faces and the hi-side of their right faces.
@@ -386,9 +374,24 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
         store(r, o);
         if (r + 1 < r1) consume(r + 3 - r0, cur);
     };
+    // The first batch's strip edges are loaded before the ring's first rows are
+    // waited for, so that the two latencies of the march's start overlap.
+    batch(r0);
+    consume(0, R1);  // row r0-1
+    consume(1, R0);  // row r0
+    {
+        const FaceT<float2> f = face_t<0, M, MASKED>(R1, R0, kp);
+        yT0 = f.f0;
+        yT1 = f.f1;
+        yT2 = A::add(f.f2, f.corr_hi);
+        if constexpr (RUN) {
+            if (r0 == 0) lg.out_y = lfma(neg(f.f0), vmask, lg.out_y);
+        }
+    }
+    consume(2, R1);  // row r0+1
     for (int rb = r0; rb < r1; rb += kBatch) {
         flush_ledger();
-        batch(rb);
+        if (rb != r0) batch(rb);
         const int re = min(rb + kBatch, r1);
         for (int r = rb; r < re; r += 2) {
             row(r, r - rb, R0, R1);

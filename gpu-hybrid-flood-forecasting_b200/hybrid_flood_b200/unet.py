@@ -87,6 +87,24 @@ def make_activation(name: str) -> nn.Module:
     return _ACTIVATIONS[key]()
 
 
+# Inference with cuDNN's fused convolution + bias + ReLU (and + add + ReLU):
+# used when no gradient is needed, on CUDA channels-last tensors with ReLU.
+# SWE_UNET_FUSED=0 keeps the separate bias/activation pass.
+_FUSED = {"on": __import__("os").environ.get("SWE_UNET_FUSED", "1") != "0"}
+
+
+def _fused_ok(x: torch.Tensor) -> bool:
+    return (_FUSED["on"] and not torch.is_grad_enabled() and x.is_cuda and x.dim() == 4
+            and x.dtype in (torch.bfloat16, torch.float16, torch.float32)
+            and x.is_contiguous(memory_format=torch.channels_last))
+
+
+def _conv_relu(conv: nn.Conv2d, x: torch.Tensor) -> torch.Tensor:
+    """relu(conv(x) + bias) in one cuDNN call."""
+    return torch.cudnn_convolution_relu(x, conv.weight, conv.bias, list(conv.stride), list(conv.padding),
+                                        list(conv.dilation), conv.groups)
+
+
 class ConvPair(nn.Module):
     """Two same-size k×k convolutions, each followed by the activation."""
 
@@ -99,9 +117,24 @@ class ConvPair(nn.Module):
         self.relu = activation.lower() == "relu"
 
     def forward(self, x: torch.Tensor) -> torch.Tensor:
+        if self.relu and _fused_ok(x):
+            return _conv_relu(self.conv_2, _conv_relu(self.conv_1, x))
         if self.relu:
             return conv_bias_act(self.conv_2, conv_bias_act(self.conv_1, x, True), True)
         return self.activation_2(self.conv_2(self.activation_1(self.conv_1(x))))
+
+    def forward_split(self, up: torch.Tensor, skip: torch.Tensor) -> torch.Tensor:
+        """forward(cat(up, skip)) without the concatenation: conv_1's weight is split
+        along its input channels, conv(up, W_up) is computed first and added,
+        with the bias and ReLU, inside the fused convolution over the skip."""
+        c = up.shape[1]
+        w = self.conv_1.weight
+        z = F.conv2d(up, w[:, :c].contiguous(memory_format=torch.channels_last), None, self.conv_1.stride,
+                     self.conv_1.padding)
+        y = torch.cudnn_convolution_add_relu(skip, w[:, c:].contiguous(memory_format=torch.channels_last), z, 1.0,
+                                             self.conv_1.bias, list(self.conv_1.stride), list(self.conv_1.padding),
+                                             list(self.conv_1.dilation), self.conv_1.groups)
+        return _conv_relu(self.conv_2, y)
 
 
 def pad_same_stride2(x: torch.Tensor) -> torch.Tensor:
@@ -156,7 +189,10 @@ class ResidualUNet(nn.Module):
             x = conv_bias_act(up, x, False)
             if x.shape[-2:] != skip.shape[-2:]:
                 x = F.interpolate(x, size=skip.shape[-2:], mode="bilinear", align_corners=False)
-            x = dec(torch.cat((x, skip), dim=1))
+            if dec.relu and _fused_ok(x) and _fused_ok(skip):
+                x = dec.forward_split(x, skip)
+            else:
+                x = dec(torch.cat((x, skip), dim=1))
         return conv_bias_act(self.residual_head, x, False)
 
 

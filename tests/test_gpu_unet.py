@@ -58,3 +58,22 @@ def test_fused_epilogue_bf16_and_odd_channels(cuda_device):
                                    _stream(cuda_device))
         assert rc == 0
         torch.testing.assert_close(t.float(), want, rtol=1e-2 if dt == torch.bfloat16 else 1e-6, atol=1e-2)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
+def test_cudnn_fused_inference_matches_the_separate_epilogue(cuda_device, dtype):
+    """Inference through cuDNN's fused convolution + bias + ReLU, with the decoder's
+    skip concatenation replaced by two convolutions on the split weight summed
+    inside the fused call, equals the path with the separate epilogue pass."""
+    from hybrid_flood_b200 import unet
+
+    torch.backends.cudnn.allow_tf32 = False
+    net = _net(2).to(cuda_device, dtype=dtype, memory_format=torch.channels_last).eval()
+    x = torch.randn(3, 5, 40, 52, device=cuda_device).to(dtype).contiguous(memory_format=torch.channels_last)
+    with torch.no_grad():
+        unet._FUSED["on"] = False
+        want = net(x).float()
+        unet._FUSED["on"] = True
+        got = net(x).float()
+    rel = float((got - want).norm() / want.norm())
+    assert rel < (1e-5 if dtype == torch.float32 else 2e-2), rel
