@@ -187,15 +187,14 @@ class ClockSampler:
             return
         nv = self._nv
         taken = 0
-        while taken < 1000 and not event.query():
+        while taken < 1000 and not event.query():  # each sample starts while the region runs
             try:
                 mhz = float(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
                 rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self._h))
             except Exception:  # noqa: BLE001
                 return
-            if not event.query():  # keep only samples taken before the region ended
-                self.samples.append((time.perf_counter(), mhz, rs))
-                taken += 1
+            self.samples.append((time.perf_counter(), mhz, rs))
+            taken += 1
 
     def mark_end(self):
         self.window = (self.window[0], time.perf_counter())
@@ -385,7 +384,7 @@ def _ensemble(args, dev, rank: int, world: int):
     states = ens.initial_states(depths)
     ens.advance_(states, 50)  # spin-up
     tune_states = [type(s)(*(t.clone() for t in s)) for s in states]
-    best = ens.autotune(tune_states, candidates=(32, 64, 128, 256), steps=50, cache=None)
+    best = ens.autotune(tune_states, candidates=(48, 64, 96, 128, 160, 192, 256, 320), steps=50, cache=None)
     del tune_states
     ens.advance_(states, 50)  # warm-up (graph capture)
     if world > 1:

@@ -104,6 +104,7 @@ struct Control {
     int64_t out_plane;            // rows * cols
     double ledger[6];             // volume0, volume, rain_in, outflow, clip_gain, mask_loss
     int defer_plan;               // 1: the fold leaves maxinv (NaN as +inf) for plan_kernel to use
+    int rain_seg;                 // hyetograph segment of the last planned step (a search hint)
 };
 
 struct Partial {
@@ -269,18 +270,35 @@ __device__ __forceinline__ FaceFlux face_flux(const Cell& lo, const Cell& hi, co
 // ---------------------------------------------------------------------------
 // np.interp(t, times, rates, left=default, right=default) in float64 with
 // separately rounded operations (shallow_water_2d.py:254-264).
-__device__ inline double rain_rate_unscaled(const DomainDev& d, double t) {
+// `seg` (may be null) caches the segment of the previous call: a run's clock only
+// advances, so the segment is usually the same or the next one, and checking
+// those two replaces the binary search's chain of dependent loads.  A cached
+// segment is used only when it contains t (rain_t[lo] <= t < rain_t[lo + 1]),
+// where it is the one the search finds.
+__device__ inline double rain_rate_unscaled(const DomainDev& d, double t, int* seg = nullptr) {
     const int n = d.n_rain;
     if (n <= 0) return d.default_rain;
     const double x0 = d.rain_t[0], xn = d.rain_t[n - 1];
     if (t != t) return t;
     if (t < x0 || t > xn) return d.default_rain;
     if (n == 1 || t == xn) return d.rain_r[n - 1];
-    int lo = 0, hi = n - 1;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (d.rain_t[mid] <= t) lo = mid; else hi = mid;
+    int lo = -1;
+    if (seg) {
+        for (int cand = *seg; cand <= *seg + 1; ++cand)
+            if (cand >= 0 && cand < n - 1 && d.rain_t[cand] <= t && t < d.rain_t[cand + 1]) {
+                lo = cand;
+                break;
+            }
     }
+    if (lo < 0) {
+        lo = 0;
+        int hi = n - 1;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (d.rain_t[mid] <= t) lo = mid; else hi = mid;
+        }
+    }
+    if (seg) *seg = lo;
     const double xj = d.rain_t[lo], yj = d.rain_r[lo];
     if (t == xj) return yj;
     const double xj1 = d.rain_t[lo + 1], yj1 = d.rain_r[lo + 1];
@@ -293,15 +311,15 @@ __device__ inline double rain_rate_unscaled(const DomainDev& d, double t) {
     return v;
 }
 
-__device__ inline double rain_rate(const DomainDev& d, double t) {
-    return __dmul_rn(d.rain_scale, rain_rate_unscaled(d, t));
+__device__ inline double rain_rate(const DomainDev& d, double t, int* seg = nullptr) {
+    return __dmul_rn(d.rain_scale, rain_rate_unscaled(d, t, seg));
 }
 
 // Float32 scalars of a step of length dt starting at t.
-__device__ inline StepScalars step_scalars(const DomainDev& d, double dt, double t) {
+__device__ inline StepScalars step_scalars(const DomainDev& d, double dt, double t, int* seg = nullptr) {
     StepScalars s;
     s.dt = __double2float_rn(dt);
-    s.dt_rain = __double2float_rn(__dmul_rn(dt, rain_rate(d, t)));
+    s.dt_rain = __double2float_rn(__dmul_rn(dt, rain_rate(d, t, seg)));
     s.dt_g = __double2float_rn(__dmul_rn(dt, d.g));
     return s;
 }
@@ -337,7 +355,7 @@ __device__ inline void plan_next(const DomainDev& d, Control& c) {
     const double remain = __dsub_rn(target, c.t);
     if (remain < dt) dt = remain;
     c.dt = dt;
-    c.s = step_scalars(d, dt, c.t);
+    c.s = step_scalars(d, dt, c.t, &c.rain_seg);
     c.reach = (__dadd_rn(c.t, dt) >= __dsub_rn(target, 1.0e-7)) ? c.idx : -1;
     // Without output buffers (advance, advance_to) nothing is recorded.
     c.snap = c.out_h ? c.reach : -1;
@@ -453,11 +471,32 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     // Fixed-order fold of all CTA partials: thread t folds partials t, t+T, ...
     Accum a;
     a.zero();
-    const volatile Partial* vp = parts;
-    for (int b = threadIdx.x; b < nparts; b += THREADS) {
-        a.maxinv = nan_max(a.maxinv, vp[b].maxinv);
-        a.vol += vp[b].vol; a.rain += vp[b].rain; a.outflow += vp[b].outflow;
-        a.clip += vp[b].clip; a.mask += vp[b].mask;
+    // A batch of this thread's partials is loaded from the L2 (.cg: the other
+    // CTAs' writes are visible there after the fence) with every load in flight
+    // at once, then folded in the same fixed order.
+    constexpr int kPer = 8;
+    for (int base = threadIdx.x; base < nparts; base += kPer * THREADS) {
+        Partial buf[kPer];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int b = base + j * THREADS;
+            if (b < nparts) {
+                buf[j].maxinv = __ldcg(&parts[b].maxinv);
+                buf[j].vol = __ldcg(&parts[b].vol);
+                buf[j].rain = __ldcg(&parts[b].rain);
+                buf[j].outflow = __ldcg(&parts[b].outflow);
+                buf[j].clip = __ldcg(&parts[b].clip);
+                buf[j].mask = __ldcg(&parts[b].mask);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            if (base + j * THREADS < nparts) {
+                a.maxinv = nan_max(a.maxinv, buf[j].maxinv);
+                a.vol += buf[j].vol; a.rain += buf[j].rain; a.outflow += buf[j].outflow;
+                a.clip += buf[j].clip; a.mask += buf[j].mask;
+            }
+        }
     }
     __syncthreads();
     a.maxinv = warp_max(a.maxinv);
