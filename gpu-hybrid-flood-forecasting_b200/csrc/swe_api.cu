@@ -130,7 +130,7 @@ struct swe_domain {
     // CUDA graph of kChunk run-mode steps starting from ping buffer 0, and the
     // inputs it was captured with (a change of any of them re-captures it).
     cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t chunk_graph = nullptr;
+    cudaGraphExec_t chunk_graph[2][33] = {};  // [start buffer parity][steps 1..32]
     const Partial* chunk_graph_parts = nullptr;
     double chunk_graph_rain_scale = 0.0;
     int chunk_graph_rows = 0;
@@ -395,55 +395,60 @@ StepLaunch run_launch(const swe_domain* d, const Plan& pl, int64_t k) {
     return sl;
 }
 
-// The kChunk-step graph from ping buffer 0, captured on a private stream (the
-// caller's stream may be the legacy default stream, which cannot be captured).
-// Its kernel parameters hold the domain record by value, so a change of the
-// partials buffer, the rain scale or the plan re-captures it.
-int chunk_graph(swe_domain* d, const Plan& pl, cudaGraphExec_t* out) {
-    if (d->chunk_graph && d->chunk_graph_parts == d->parts && d->chunk_graph_rain_scale == d->dd.rain_scale &&
-        d->chunk_graph_rows == pl.rows_per_warp) {
-        *out = d->chunk_graph;
-        return SWE_OK;
+// The graph of `len` (1..kChunk) run-mode steps starting from ping buffer
+// `par`, captured on a private stream (the caller's stream may be the legacy
+// default stream, which cannot be captured) on first use.  Its kernel
+// parameters hold the domain record by value, so a change of the partials
+// buffer, the rain scale or the plan re-captures every graph.
+void drop_chunk_graphs(swe_domain* d) {
+    for (auto& row : d->chunk_graph)
+        for (auto& g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+}
+
+int chunk_graph(swe_domain* d, const Plan& pl, int par, int len, cudaGraphExec_t* out) {
+    if (d->chunk_graph_parts != d->parts || d->chunk_graph_rain_scale != d->dd.rain_scale ||
+        d->chunk_graph_rows != pl.rows_per_warp) {
+        drop_chunk_graphs(d);
+        d->chunk_graph_parts = d->parts;
+        d->chunk_graph_rain_scale = d->dd.rain_scale;
+        d->chunk_graph_rows = pl.rows_per_warp;
     }
-    if (d->chunk_graph) {
-        cudaGraphExecDestroy(d->chunk_graph);
-        d->chunk_graph = nullptr;
+    cudaGraphExec_t& slot = d->chunk_graph[par][len];
+    if (slot) {
+        *out = slot;
+        return SWE_OK;
     }
     if (!d->cap_stream) SWE_CK(cudaStreamCreateWithFlags(&d->cap_stream, cudaStreamNonBlocking));
     SWE_CK(cudaStreamBeginCapture(d->cap_stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < kChunk; ++k) launch_step(d, pl, run_launch(d, pl, k), true, d->cap_stream);
+    for (int k = 0; k < len; ++k) launch_step(d, pl, run_launch(d, pl, par + k), true, d->cap_stream);
     cudaGraph_t g = nullptr;
     SWE_CK(cudaStreamEndCapture(d->cap_stream, &g));
-    const cudaError_t err = cudaGraphInstantiate(&d->chunk_graph, g, 0);
+    const cudaError_t err = cudaGraphInstantiate(&slot, g, 0);
     cudaGraphDestroy(g);
     if (err != cudaSuccess) {
-        d->chunk_graph = nullptr;
+        slot = nullptr;
         return fail(SWE_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(err));
     }
-    d->chunk_graph_parts = d->parts;
-    d->chunk_graph_rain_scale = d->dd.rain_scale;
-    d->chunk_graph_rows = pl.rows_per_warp;
-    *out = d->chunk_graph;
+    *out = slot;
     return SWE_OK;
 }
 
-// Enqueue steps k0 .. k0+n-1 of the current run: whole kChunk-step graphs where
-// the step index is even and a whole chunk remains, single launches elsewhere.
+// Enqueue steps k0 .. k0+n-1 of the current run as graphs of up to kChunk steps.
 int enqueue_run_steps(swe_domain* d, int64_t k0, int64_t n, cudaStream_t st) {
     const Plan pl = make_plan(d, d->run_vec, true);
     int64_t k = k0;
     const int64_t end = k0 + n;
     while (k < end) {
-        if ((k & 1) == 0 && end - k >= kChunk) {
-            cudaGraphExec_t g = nullptr;
-            const int rc = chunk_graph(d, pl, &g);
-            if (rc) return rc;
-            SWE_CK(cudaGraphLaunch(g, st));
-            k += kChunk;
-        } else {
-            launch_step(d, pl, run_launch(d, pl, k), true, st);
-            ++k;
-        }
+        const int len = (int)std::min<int64_t>(kChunk, end - k);
+        cudaGraphExec_t g = nullptr;
+        const int rc = chunk_graph(d, pl, (int)(k & 1), len, &g);
+        if (rc) return rc;
+        SWE_CK(cudaGraphLaunch(g, st));
+        k += len;
     }
     SWE_CK(cudaGetLastError());
     return SWE_OK;
@@ -526,7 +531,7 @@ void free_domain(swe_domain* d) {
         if (d->poll_ev[i]) cudaEventDestroy(d->poll_ev[i]);
         if (d->time_ev[i]) cudaEventDestroy(d->time_ev[i]);
     }
-    if (d->chunk_graph) cudaGraphExecDestroy(d->chunk_graph);
+    drop_chunk_graphs(d);
     if (d->cap_stream) cudaStreamDestroy(d->cap_stream);
     cudaFree(d->snap_dev);
     if (d->copy_stream) cudaStreamDestroy(d->copy_stream);
