@@ -537,8 +537,13 @@ def _hybrid(args, dev):
     # FLOPs of one corrector forward (convolutions and transposed convolutions, 2 per MAC)
     from torch.utils.flop_counter import FlopCounterMode
 
+    from hybrid_flood_b200 import unet as unet_mod
+
+    fused_on = unet_mod._FUSED["on"]
+    unet_mod._FUSED["on"] = False  # the counter sees torch convolutions, not cuDNN's fused calls (same math)
     with torch.no_grad(), FlopCounterMode(display=False) as fc:
         net(feats)
+    unet_mod._FUSED["on"] = fused_on
     net_flops = float(fc.get_total_flops())
     tf_peak, tf_kind = _tensor_peak()
     cells = M * S * S

@@ -421,7 +421,10 @@ __device__ __forceinline__ void after_plan(Control& c) {
     if (c.done && c.done_counter) atomicAdd(c.done_counter, 1u);
 }
 
-template <int THREADS>
+// PER: partials a thread of the last CTA loads before folding them (8 covers a
+// one-wave grid in one batch; the ensemble kernel, which folds each member's few
+// CTAs and has no registers to spare, uses 1).
+template <int THREADS, int PER = 8>
 __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts, Accum acc,
                                 bool init, int part = -1, int nparts = -1) {
     // One partial per CTA of this domain: by default the launch's CTAs; the
@@ -474,7 +477,7 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     // A batch of this thread's partials is loaded from the L2 (.cg: the other
     // CTAs' writes are visible there after the fence) with every load in flight
     // at once, then folded in the same fixed order.
-    constexpr int kPer = 8;
+    constexpr int kPer = PER;
     for (int base = threadIdx.x; base < nparts; base += kPer * THREADS) {
         Partial buf[kPer];
 #pragma unroll

@@ -518,7 +518,7 @@ ensemble_step_kernel(const MemberDev* __restrict__ members, const int2* __restri
         a.outflow = acc.outflow;
         a.clip = acc.clip;
         a.mask = acc.mask;
-        finish_run_step<THREADS>(md.d, md.ctl, md.parts, a, false, item.y, md.ncta);
+        finish_run_step<THREADS, 1>(md.d, md.ctl, md.parts, a, false, item.y, md.ncta);
     }
 }
 
@@ -573,7 +573,7 @@ ensemble_step_kernel_p(const __grid_constant__ EnsParams p) {
         a.outflow = acc.outflow;
         a.clip = acc.clip;
         a.mask = acc.mask;
-        finish_run_step<THREADS>(md.d, md.ctl, md.parts, a, false, slot, md.ncta);
+        finish_run_step<THREADS, 1>(md.d, md.ctl, md.parts, a, false, slot, md.ncta);
         __syncthreads();  // the fold's shared scratch is free before the next item
     }
 }
