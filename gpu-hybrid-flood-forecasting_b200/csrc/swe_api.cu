@@ -100,7 +100,9 @@ struct swe_domain {
     Control* ctl_scratch = nullptr;  // standalone reductions (device)
     Control* ctl_host = nullptr;     // pinned poll slots [2]
     Partial* parts = nullptr;
-    int parts_cap = 0;
+    int parts_cap = 0;            // step CTAs' ledger slots (kept over a run)
+    Partial* rparts = nullptr;     // partials of the standalone CFL/volume reductions
+    int rparts_cap = 0;
     float* ping[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int64_t ppitch = 0;
     float* times_dev = nullptr;
@@ -264,9 +266,9 @@ int reduce_blocks(const swe_domain* d) {
 void launch_reduce(const swe_domain* d, const StateView& s, Control* ctl, cudaStream_t st) {
     const int blocks = reduce_blocks(d);
     if (d->arith == SWE_ARITH_FAST)
-        reduce_kernel<FastMath, kThreads><<<blocks, kThreads, 0, st>>>(d->dd, s, ctl, d->parts);
+        reduce_kernel<FastMath, kThreads><<<blocks, kThreads, 0, st>>>(d->dd, s, ctl, d->rparts);
     else
-        reduce_kernel<ExactMath, kThreads><<<blocks, kThreads, 0, st>>>(d->dd, s, ctl, d->parts);
+        reduce_kernel<ExactMath, kThreads><<<blocks, kThreads, 0, st>>>(d->dd, s, ctl, d->rparts);
 }
 
 int choose_vec(const void* const* ptrs, int n, int64_t pitch_a, int64_t pitch_b) {
@@ -279,7 +281,21 @@ int choose_vec(const void* const* ptrs, int n, int64_t pitch_a, int64_t pitch_b)
     return 1;
 }
 
+// Partials of the reductions (reduce_kernel); separate from the step slots so that
+// a CFL query in the middle of a resident run leaves its ledger intact.
+int ensure_rparts(swe_domain* d) {
+    const int blocks = reduce_blocks(d);
+    if (blocks <= d->rparts_cap) return SWE_OK;
+    if (d->rparts) cudaFree(d->rparts);
+    d->rparts = nullptr;
+    SWE_CK(cudaMalloc(&d->rparts, sizeof(Partial) * (size_t)blocks));
+    d->rparts_cap = blocks;
+    return SWE_OK;
+}
+
 int ensure_parts(swe_domain* d, int blocks) {
+    const int rrc = ensure_rparts(d);
+    if (rrc) return rrc;
     if (blocks <= d->parts_cap) return SWE_OK;
     if (d->parts) cudaFree(d->parts);
     d->parts = nullptr;
@@ -373,6 +389,15 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
     SWE_CK(cudaMemcpyAsync(d->ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, st));
     StateView v0{d->ping[0][0], d->ping[0][1], d->ping[0][2], d->ppitch};
     launch_reduce(d, v0, d->ctl, st);
+    SWE_CK(cudaGetLastError());
+    // The step CTAs' ledger slots start the run at zero (after the reduction's own fold).
+    SWE_CK(cudaMemsetAsync(d->parts, 0, sizeof(Partial) * (size_t)d->parts_cap, st));
+    return SWE_OK;
+}
+
+// The run's ledger into the control block from the step CTAs' slots.
+int fold_ledger(swe_domain* d, int nslots, cudaStream_t st) {
+    ledger_fold_kernel<kThreads><<<1, kThreads, 0, st>>>(d->dd, d->ctl, d->parts, nslots);
     SWE_CK(cudaGetLastError());
     return SWE_OK;
 }
@@ -496,6 +521,8 @@ int run_driver(swe_domain* d, StateView init, const float* times_host, int n_tim
         d->timed_steps = launched;
         d->timed_valid = true;
     }
+    rc = fold_ledger(d, pl.blocks, st);
+    if (rc) return rc;
     SWE_CK(cudaStreamSynchronize(st));
     SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
     const Control& c = d->ctl_host[0];
@@ -519,6 +546,7 @@ void free_domain(swe_domain* d) {
     cudaFree(d->ctl_scratch);
     if (d->ctl_host) cudaFreeHost(d->ctl_host);
     cudaFree(d->parts);
+    cudaFree(d->rparts);
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 3; ++f) cudaFree(d->ping[b][f]);
     cudaFree(d->times_dev);
@@ -590,6 +618,7 @@ struct swe_ensemble {
     // Member table in the kernel's parameter space (up to kEnsParamMembers
     // members; SWE_ENS_PARAM_TABLE=0 keeps the table in global memory).
     std::unique_ptr<EnsParams> params;
+    std::vector<int> member_ncta;  // step CTAs (ledger slots) of each member
 };
 
 namespace {
@@ -662,6 +691,8 @@ int ens_rebuild(swe_ensemble* e) {
         x.rows_per_warp = R;
         x.ncta = ncta;
         for (int c = 0; c < ncta; ++c) items.push_back(make_int2((int)m, c));
+        e->member_ncta.resize(e->doms.size());
+        e->member_ncta[m] = ncta;
     }
     if ((int)md.size() > e->members_cap) {
         cudaFree(e->members_dev);
@@ -727,6 +758,10 @@ int ens_graph(swe_ensemble* e, int K) {
 int ens_collect(swe_ensemble* e, float* const* h, float* const* hu, float* const* hv, const int64_t* pitch,
                 swe_run_result* results, cudaStream_t st, bool need_target) {
     const int n = (int)e->doms.size();
+    for (int m = 0; m < n; ++m) {
+        const int rc = fold_ledger(e->doms[m], e->member_ncta[m], st);
+        if (rc) return rc;
+    }
     SWE_CK(cudaStreamSynchronize(st));
     int status = SWE_OK;
     for (int m = 0; m < n; ++m) {
@@ -1382,6 +1417,8 @@ int swe_run_host(swe_domain_t d, const float* h0, const float* hu0, const float*
         }
         ++chunk;
     }
+    rc = fold_ledger(d, pl.blocks, st);
+    if (rc) return rc;
     SWE_CK(cudaStreamSynchronize(st));
     SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
     const Control& c = d->ctl_host[0];
@@ -1477,6 +1514,8 @@ int swe_resident_store(swe_domain_t d, float* h, float* hu, float* hv, int64_t p
         rc = copy_plane(outs[f], pitch, d->ping[fb][f], d->ppitch, d->dd.rows, d->dd.cols, st);
         if (rc) return rc;
     }
+    rc = fold_ledger(d, make_plan(d, d->run_vec, true).blocks, st);
+    if (rc) return rc;
     SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
     SWE_CK(cudaStreamSynchronize(st));
     const Control& c = d->ctl_host[0];
@@ -2283,6 +2322,8 @@ void strip_step(swe_domain* d, int k, cudaStream_t st) {
 
 int strip_finish(swe_domain* d, float* h, float* hu, float* hv, int64_t pitch, int n_steps, swe_run_result* r,
                  cudaStream_t st) {
+    const int lrc = fold_ledger(d, make_plan(d, d->run_vec, true).blocks, st);
+    if (lrc) return lrc;
     const int fb = n_steps & 1;
     float* outs[3] = {h, hu, hv};
     for (int f = 0; f < 3; ++f) {

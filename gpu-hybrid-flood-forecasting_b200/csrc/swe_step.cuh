@@ -105,6 +105,7 @@ struct Control {
     double ledger[6];             // volume0, volume, rain_in, outflow, clip_gain, mask_loss
     int defer_plan;               // 1: the fold leaves maxinv (NaN as +inf) for plan_kernel to use
     int rain_seg;                 // hyetograph segment of the last planned step (a search hint)
+    unsigned max_bits;            // the step's CFL maximum as float bits (atomicMax), 0 between steps
 };
 
 struct Partial {
@@ -421,22 +422,13 @@ __device__ __forceinline__ void after_plan(Control& c) {
     if (c.done && c.done_counter) atomicAdd(c.done_counter, 1u);
 }
 
-// PER: partials a thread of the last CTA loads before folding them (8 covers a
-// one-wave grid in one batch; the ensemble kernel, which folds each member's few
-// CTAs and has no registers to spare, uses 1).
-template <int THREADS, int PER = 8>
-__device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts, Accum acc,
-                                bool init, int part = -1, int nparts = -1) {
-    // One partial per CTA of this domain: by default the launch's CTAs; the
-    // ensemble kernel passes the CTA's slot within its member instead.
-    if (part < 0) {
-        part = blockIdx.x;
-        nparts = gridDim.x;
-    }
+// CTA-wide reduction of a thread's accumulators (fixed order) into the CTA's
+// totals, valid on thread 0.
+template <int THREADS>
+__device__ __forceinline__ Partial cta_reduce(Accum acc) {
     constexpr int W = THREADS / kWarp;
     __shared__ float s_max[W];
     __shared__ double s_sum[5][W];
-    __shared__ bool s_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     acc.maxinv = warp_max(acc.maxinv);
     acc.vol = warp_sum(acc.vol);
@@ -453,8 +445,8 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
         s_sum[4][warp] = acc.mask;
     }
     __syncthreads();
+    Partial p{};
     if (threadIdx.x == 0) {
-        Partial p;
         p.maxinv = s_max[0];
         p.vol = s_sum[0][0]; p.rain = s_sum[1][0]; p.outflow = s_sum[2][0];
         p.clip = s_sum[3][0]; p.mask = s_sum[4][0];
@@ -463,6 +455,75 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
             p.vol += s_sum[0][w]; p.rain += s_sum[1][w]; p.outflow += s_sum[2][w];
             p.clip += s_sum[3][w]; p.mask += s_sum[4][w];
         }
+    }
+    __syncthreads();  // s_max / s_sum are free again
+    return p;
+}
+
+// End of a step (or of the reduction that starts a run) for one CTA.
+//
+// Step: the CTA's ledger terms go into its own slot of `parts` (the volume
+// replaced, the other terms added: each slot sums its cells over the whole run
+// in a fixed order, and ledger_fold_kernel adds the slots when the run's
+// results are read); its CFL maximum goes into the control block by an
+// atomic maximum of the float bits (a NaN volume, i.e. a non-finite state in
+// the CTA, counts as NaN, which beats every finite bit pattern); the last CTA
+// of the domain to arrive takes the maximum, advances the clock and plans the
+// next step.  The serial tail of a step is thus one ticket, one exchange and
+// the plan: the ledger sums, which no step needs, are off that path.
+//
+// Start of a run (init): the reduction's CTA partials are folded by the last
+// CTA in a fixed order into volume0 and the first CFL maximum.
+//
+// PER: partials a thread of the last CTA loads before folding them in init.
+template <int THREADS, int PER = 8>
+__device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts, Accum acc,
+                                bool init, int part = -1, int nparts = -1) {
+    // One slot per CTA of this domain: by default the launch's CTAs; the
+    // ensemble kernel passes the CTA's slot within its member instead.
+    if (part < 0) {
+        part = blockIdx.x;
+        nparts = gridDim.x;
+    }
+    __shared__ bool s_last;
+    const Partial p = cta_reduce<THREADS>(acc);
+    if (!init) {
+        if (threadIdx.x != 0) return;
+        Partial& q = parts[part];
+        q.vol = p.vol;
+        q.rain += p.rain;
+        q.outflow += p.outflow;
+        q.clip += p.clip;
+        q.mask += p.mask;
+        const unsigned bits =
+            (p.vol == p.vol) ? (__float_as_uint(p.maxinv) & 0x7fffffffu) : 0x7fc00000u;
+        atomicMax(&ctl->max_bits, bits);
+        __threadfence();
+        const unsigned ticket = atomicAdd(&ctl->counter, 1u);
+        if (ticket != (unsigned)nparts - 1) return;
+        __threadfence();
+        const float mx = __uint_as_float(atomicExch(&ctl->max_bits, 0u));
+        Control c = *ctl;
+        c.t = __dadd_rn(c.t, c.dt);
+        c.steps += 1;
+        if (c.reach >= 0) c.idx = c.reach + 1;
+        c.maxinv = mx;
+        c.counter = 0;
+        c.max_bits = 0;
+        if (c.defer_plan) {
+            // A row strip: the CFL maximum of the whole domain is formed across the
+            // strips first (NaN kept as +inf so that a maximum carries it), then
+            // plan_kernel plans the step.
+            if (!(mx == mx)) c.maxinv = INFINITY;
+        } else {
+            plan_next(d, c);
+            after_plan(c);
+        }
+        *ctl = c;
+        __threadfence();
+        return;
+    }
+    if (threadIdx.x == 0) {
         parts[part] = p;
         __threadfence();
         const unsigned ticket = atomicAdd(&ctl->counter, 1u);
@@ -471,12 +532,11 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    // Fixed-order fold of all CTA partials: thread t folds partials t, t+T, ...
+    // Fixed-order fold of all CTA partials: thread t folds partials t, t+T, ...,
+    // a batch of them loaded from the L2 (.cg: the other CTAs' writes are
+    // visible there after the fence) with every load in flight at once.
     Accum a;
     a.zero();
-    // A batch of this thread's partials is loaded from the L2 (.cg: the other
-    // CTAs' writes are visible there after the fence) with every load in flight
-    // at once, then folded in the same fixed order.
     constexpr int kPer = PER;
     for (int base = threadIdx.x; base < nparts; base += kPer * THREADS) {
         Partial buf[kPer];
@@ -501,56 +561,26 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
             }
         }
     }
-    __syncthreads();
-    a.maxinv = warp_max(a.maxinv);
-    a.vol = warp_sum(a.vol); a.rain = warp_sum(a.rain); a.outflow = warp_sum(a.outflow);
-    a.clip = warp_sum(a.clip); a.mask = warp_sum(a.mask);
-    if (lane == 0) {
-        s_max[warp] = a.maxinv;
-        s_sum[0][warp] = a.vol; s_sum[1][warp] = a.rain; s_sum[2][warp] = a.outflow;
-        s_sum[3][warp] = a.clip; s_sum[4][warp] = a.mask;
-    }
-    __syncthreads();
+    const Partial t = cta_reduce<THREADS>(a);
     if (threadIdx.x != 0) return;
-    float mx = s_max[0];
-    double vol = s_sum[0][0], rain = s_sum[1][0], outflow = s_sum[2][0], clip = s_sum[3][0],
-           mask = s_sum[4][0];
-    for (int w = 1; w < W; ++w) {
-        mx = nan_max(mx, s_max[w]);
-        vol += s_sum[0][w]; rain += s_sum[1][w]; outflow += s_sum[2][w];
-        clip += s_sum[3][w]; mask += s_sum[4][w];
-    }
-    // A NaN volume means a non-finite state somewhere (the paired march folds
-    // its non-finite inverse dts into the volume partials): report it as a NaN
-    // CFL maximum, the form plan_next tests.
-    if (!(vol == vol)) mx = __int_as_float(0x7fffffff);
+    float mx = t.maxinv;
+    // A NaN volume means a non-finite state somewhere: report it as a NaN CFL
+    // maximum, the form plan_next tests.
+    if (!(t.vol == t.vol)) mx = __int_as_float(0x7fffffff);
     Control c = *ctl;
     const double area = d.dx * d.dy;
-    if (init) {
-        c.t = c.t_start;
-        c.idx = 1;
-        c.steps = 0;
-        c.done = 0;
-        c.status = 0;
-        c.ledger[0] = vol * area;
-        c.ledger[1] = vol * area;
-        c.ledger[2] = c.ledger[3] = c.ledger[4] = c.ledger[5] = 0.0;
-    } else {
-        c.t = __dadd_rn(c.t, c.dt);
-        c.steps += 1;
-        if (c.reach >= 0) c.idx = c.reach + 1;
-        c.ledger[1] = vol * area;
-        c.ledger[2] += rain * area;
-        c.ledger[3] += outflow;
-        c.ledger[4] += clip * area;
-        c.ledger[5] += mask * area;
-    }
+    c.t = c.t_start;
+    c.idx = 1;
+    c.steps = 0;
+    c.done = 0;
+    c.status = 0;
+    c.ledger[0] = t.vol * area;
+    c.ledger[1] = t.vol * area;
+    c.ledger[2] = c.ledger[3] = c.ledger[4] = c.ledger[5] = 0.0;
     c.maxinv = mx;
     c.counter = 0;
+    c.max_bits = 0;
     if (c.defer_plan) {
-        // A row strip: the CFL maximum of the whole domain is formed across the
-        // strips first (NaN kept as +inf so that a maximum carries it), then
-        // plan_kernel plans the step.
         if (!(mx == mx)) c.maxinv = INFINITY;
     } else {
         plan_next(d, c);
@@ -558,6 +588,28 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     }
     *ctl = c;
     __threadfence();
+}
+
+// The run's ledger from the step CTAs' slots (one CTA, fixed order): the stored
+// volume of the last step and the rain, outflow, clip and mask terms summed over
+// the run.  With no step taken the volume stays the initial one.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) ledger_fold_kernel(const DomainDev d, Control* ctl, const Partial* parts,
+                                                             int nslots) {
+    Accum a;
+    a.zero();
+    for (int b = threadIdx.x; b < nslots; b += THREADS) {
+        a.vol += parts[b].vol; a.rain += parts[b].rain; a.outflow += parts[b].outflow;
+        a.clip += parts[b].clip; a.mask += parts[b].mask;
+    }
+    const Partial t = cta_reduce<THREADS>(a);
+    if (threadIdx.x != 0) return;
+    const double area = d.dx * d.dy;
+    ctl->ledger[1] = ctl->steps > 0 ? t.vol * area : ctl->ledger[0];
+    ctl->ledger[2] = t.rain * area;
+    ctl->ledger[3] = t.outflow;
+    ctl->ledger[4] = t.clip * area;
+    ctl->ledger[5] = t.mask * area;
 }
 
 // Plans the next step of a row strip from the domain-wide CFL maximum now in
