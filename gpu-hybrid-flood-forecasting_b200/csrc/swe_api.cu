@@ -48,6 +48,7 @@ int fail(int code, const std::string& msg) {
     } while (0)
 
 constexpr int kThreads = 128;
+constexpr int kWarpsPerCta = kThreads / kWarp;
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
@@ -99,8 +100,8 @@ struct swe_domain {
     Control* ctl = nullptr;          // run control (device)
     Control* ctl_scratch = nullptr;  // standalone reductions (device)
     Control* ctl_host = nullptr;     // pinned poll slots [2]
-    Partial* parts = nullptr;
-    int parts_cap = 0;            // step CTAs' ledger slots (kept over a run)
+    LedgerSlot* slots = nullptr;  // step warps' ledger slots (kept over a run)
+    int slots_cap = 0;            // in CTAs (kWarpsPerCta slots each)
     Partial* rparts = nullptr;     // partials of the standalone CFL/volume reductions
     int rparts_cap = 0;
     float* ping[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -133,7 +134,7 @@ struct swe_domain {
     // inputs it was captured with (a change of any of them re-captures it).
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t chunk_graph[2][33] = {};  // [start buffer parity][steps 1..32]
-    const Partial* chunk_graph_parts = nullptr;
+    const LedgerSlot* chunk_graph_slots = nullptr;
     double chunk_graph_rain_scale = 0.0;
     int chunk_graph_rows = 0;
     // Resident run (swe_resident_*): state kept in the ping buffers between calls.
@@ -293,14 +294,16 @@ int ensure_rparts(swe_domain* d) {
     return SWE_OK;
 }
 
+// Ledger slots of the run-mode steps for `blocks` CTAs (one per warp), and the
+// reduction partials.
 int ensure_parts(swe_domain* d, int blocks) {
     const int rrc = ensure_rparts(d);
     if (rrc) return rrc;
-    if (blocks <= d->parts_cap) return SWE_OK;
-    if (d->parts) cudaFree(d->parts);
-    d->parts = nullptr;
-    SWE_CK(cudaMalloc(&d->parts, sizeof(Partial) * (size_t)blocks));
-    d->parts_cap = blocks;
+    if (blocks <= d->slots_cap) return SWE_OK;
+    if (d->slots) cudaFree(d->slots);
+    d->slots = nullptr;
+    SWE_CK(cudaMalloc(&d->slots, sizeof(LedgerSlot) * kWarpsPerCta * (size_t)blocks));
+    d->slots_cap = blocks;
     return SWE_OK;
 }
 
@@ -383,21 +386,20 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
     c0.out_hu = out_hu;
     c0.out_hv = out_hv;
     c0.out_plane = (int64_t)rows * cols;
-    c0.snap = -1;
-    c0.reach = -1;
     // Pageable source: the copy is staged before cudaMemcpyAsync returns.
     SWE_CK(cudaMemcpyAsync(d->ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, st));
     StateView v0{d->ping[0][0], d->ping[0][1], d->ping[0][2], d->ppitch};
     launch_reduce(d, v0, d->ctl, st);
     SWE_CK(cudaGetLastError());
-    // The step CTAs' ledger slots start the run at zero (after the reduction's own fold).
-    SWE_CK(cudaMemsetAsync(d->parts, 0, sizeof(Partial) * (size_t)d->parts_cap, st));
+    // The step warps' ledger slots start the run at zero.
+    SWE_CK(cudaMemsetAsync(d->slots, 0, sizeof(LedgerSlot) * kWarpsPerCta * (size_t)d->slots_cap, st));
     return SWE_OK;
 }
 
-// The run's ledger into the control block from the step CTAs' slots.
-int fold_ledger(swe_domain* d, int nslots, cudaStream_t st) {
-    ledger_fold_kernel<kThreads><<<1, kThreads, 0, st>>>(d->dd, d->ctl, d->parts, nslots);
+// The run's ledger into the control block from the slots of the step warps of
+// `ncta` CTAs.
+int fold_ledger(swe_domain* d, int ncta, cudaStream_t st) {
+    ledger_fold_kernel<kThreads><<<1, kThreads, 0, st>>>(d->dd, d->ctl, d->slots, ncta * kWarpsPerCta);
     SWE_CK(cudaGetLastError());
     return SWE_OK;
 }
@@ -411,10 +413,11 @@ StepLaunch run_launch(const swe_domain* d, const Plan& pl, int64_t k) {
     StepLaunch sl{};
     sl.d = d->dd;
     sl.ctl = d->ctl;
-    sl.parts = d->parts;
+    sl.slots = d->slots;
     sl.nstrips = pl.nstrips;
     sl.rows_per_warp = pl.rows_per_warp;
     const int src = (int)(k & 1);
+    sl.par = src;
     sl.in = StateView{d->ping[src][0], d->ping[src][1], d->ping[src][2], d->ppitch};
     sl.out = StateOut{d->ping[src ^ 1][0], d->ping[src ^ 1][1], d->ping[src ^ 1][2], d->ppitch};
     return sl;
@@ -435,10 +438,10 @@ void drop_chunk_graphs(swe_domain* d) {
 }
 
 int chunk_graph(swe_domain* d, const Plan& pl, int par, int len, cudaGraphExec_t* out) {
-    if (d->chunk_graph_parts != d->parts || d->chunk_graph_rain_scale != d->dd.rain_scale ||
+    if (d->chunk_graph_slots != d->slots || d->chunk_graph_rain_scale != d->dd.rain_scale ||
         d->chunk_graph_rows != pl.rows_per_warp) {
         drop_chunk_graphs(d);
-        d->chunk_graph_parts = d->parts;
+        d->chunk_graph_slots = d->slots;
         d->chunk_graph_rain_scale = d->dd.rain_scale;
         d->chunk_graph_rows = pl.rows_per_warp;
     }
@@ -462,18 +465,24 @@ int chunk_graph(swe_domain* d, const Plan& pl, int par, int len, cudaGraphExec_t
     return SWE_OK;
 }
 
-// Enqueue steps k0 .. k0+n-1 of the current run as graphs of up to kChunk steps.
-int enqueue_run_steps(swe_domain* d, int64_t k0, int64_t n, cudaStream_t st) {
+// Enqueue steps k0 .. k0+n-1 of the current run as graphs of up to kChunk
+// steps.  Every graph the steps need is captured before the first one is
+// launched, so that the stream never waits for the host in between; with
+// launch == false the graphs are only captured.
+int enqueue_run_steps(swe_domain* d, int64_t k0, int64_t n, cudaStream_t st, bool launch = true) {
     const Plan pl = make_plan(d, d->run_vec, true);
-    int64_t k = k0;
     const int64_t end = k0 + n;
-    while (k < end) {
-        const int len = (int)std::min<int64_t>(kChunk, end - k);
+    for (int64_t k = k0; k < end; k += kChunk) {
         cudaGraphExec_t g = nullptr;
-        const int rc = chunk_graph(d, pl, (int)(k & 1), len, &g);
+        const int rc = chunk_graph(d, pl, (int)(k & 1), (int)std::min<int64_t>(kChunk, end - k), &g);
+        if (rc) return rc;
+    }
+    if (!launch) return SWE_OK;
+    for (int64_t k = k0; k < end; k += kChunk) {
+        cudaGraphExec_t g = nullptr;
+        const int rc = chunk_graph(d, pl, (int)(k & 1), (int)std::min<int64_t>(kChunk, end - k), &g);
         if (rc) return rc;
         SWE_CK(cudaGraphLaunch(g, st));
-        k += len;
     }
     SWE_CK(cudaGetLastError());
     return SWE_OK;
@@ -506,7 +515,7 @@ int run_driver(swe_domain* d, StateView init, const float* times_host, int n_tim
         launched += todo;
         d->launches += todo;
         const int slot = chunk & 1;
-        SWE_CK(cudaMemcpyAsync(&d->ctl_host[slot], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+        SWE_CK(cudaMemcpyAsync(&d->ctl_host[slot], d->ctl, kControlHead, cudaMemcpyDeviceToHost, st));
         SWE_CK(cudaEventRecord(d->poll_ev[slot], st));
         if (launched >= max_steps) break;
         if (chunk > 0) {
@@ -524,7 +533,7 @@ int run_driver(swe_domain* d, StateView init, const float* times_host, int n_tim
     rc = fold_ledger(d, pl.blocks, st);
     if (rc) return rc;
     SWE_CK(cudaStreamSynchronize(st));
-    SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
+    SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, kControlHead, cudaMemcpyDeviceToHost));
     const Control& c = d->ctl_host[0];
     res->final_time_s = c.t;
     res->outputs_written = c.idx;
@@ -545,7 +554,7 @@ void free_domain(swe_domain* d) {
     cudaFree(d->ctl);
     cudaFree(d->ctl_scratch);
     if (d->ctl_host) cudaFreeHost(d->ctl_host);
-    cudaFree(d->parts);
+    cudaFree(d->slots);
     cudaFree(d->rparts);
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 3; ++f) cudaFree(d->ping[b][f]);
@@ -686,7 +695,7 @@ int ens_rebuild(swe_ensemble* e) {
             for (int f = 0; f < 3; ++f) x.buf[b][f] = d->ping[b][f];
         x.pitch = d->ppitch;
         x.ctl = d->ctl;
-        x.parts = d->parts;
+        x.slots = d->slots;
         x.nstrips = nstrips;
         x.rows_per_warp = R;
         x.ncta = ncta;
@@ -766,7 +775,7 @@ int ens_collect(swe_ensemble* e, float* const* h, float* const* hu, float* const
     int status = SWE_OK;
     for (int m = 0; m < n; ++m) {
         swe_domain* d = e->doms[m];
-        SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
+        SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, kControlHead, cudaMemcpyDeviceToHost));
         const Control& c = d->ctl_host[0];
         swe_run_result& r = results[m];
         r.final_time_s = c.t;
@@ -1095,6 +1104,9 @@ int swe_domain_create(const swe_domain_desc* desc, swe_domain_t* out) {
     dd.rain_t = d->rain;
     dd.rain_r = d->rain + q.n_rain;
     dd.n_rain = q.n_rain;
+    dd.rain_x0 = d->rain_t.front();
+    dd.rain_xn = d->rain_t.back();
+    dd.rain_yn = d->rain_r.back();
     dd.rain_scale = 1.0;
     dd.upd_lo = 0;
     dd.upd_hi = q.rows;
@@ -1258,7 +1270,7 @@ int swe_step(swe_domain_t d, const float* h, const float* hu, const float* hv, i
     sl.s.dt_rain = (float)dr;
     sl.s.dt_g = (float)dg;
     sl.ctl = nullptr;
-    sl.parts = nullptr;
+    sl.slots = nullptr;
     sl.nstrips = pl.nstrips;
     sl.rows_per_warp = pl.rows_per_warp;
     launch_step(d, pl, sl, false, static_cast<cudaStream_t>(stream));
@@ -1276,12 +1288,10 @@ int swe_max_inverse_dt(swe_domain_t d, const float* h, const float* hu, const fl
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     Control c0;
     std::memset(&c0, 0, sizeof(c0));
-    c0.snap = -1;
-    c0.reach = -1;
     SWE_CK(cudaMemcpyAsync(d->ctl_scratch, &c0, sizeof(Control), cudaMemcpyHostToDevice, st));
     launch_reduce(d, StateView{h, hu, hv, pitch}, d->ctl_scratch, st);
     SWE_CK(cudaGetLastError());
-    SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl_scratch, sizeof(Control), cudaMemcpyDeviceToHost, st));
+    SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl_scratch, kControlHead, cudaMemcpyDeviceToHost, st));
     SWE_CK(cudaStreamSynchronize(st));
     *max_inverse_dt_out = d->ctl_host[0].maxinv;
     return SWE_OK;
@@ -1403,7 +1413,7 @@ int swe_run_host(swe_domain_t d, const float* h0, const float* hu0, const float*
         launched += todo;
         d->launches += todo;
         const int slot = chunk & 1;
-        SWE_CK(cudaMemcpyAsync(&d->ctl_host[slot], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+        SWE_CK(cudaMemcpyAsync(&d->ctl_host[slot], d->ctl, kControlHead, cudaMemcpyDeviceToHost, st));
         SWE_CK(cudaEventRecord(d->poll_ev[slot], st));
         if (launched >= max_steps) break;
         if (chunk > 0) {
@@ -1420,7 +1430,7 @@ int swe_run_host(swe_domain_t d, const float* h0, const float* hu0, const float*
     rc = fold_ledger(d, pl.blocks, st);
     if (rc) return rc;
     SWE_CK(cudaStreamSynchronize(st));
-    SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
+    SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, kControlHead, cudaMemcpyDeviceToHost));
     const Control& c = d->ctl_host[0];
     SWE_CK(cudaEventRecord(d->snap_ev, st));
     rc = copy_out(std::min(c.idx, n_out), d->snap_ev);
@@ -1501,6 +1511,13 @@ int swe_resident_steps(swe_domain_t d, int32_t n_steps, void* stream) {
     return SWE_OK;
 }
 
+int swe_resident_prepare(swe_domain_t d, int32_t n_steps) {
+    if (!d) return fail(SWE_ERR_INVALID, "null domain");
+    if (!d->resident) return fail(SWE_ERR_INVALID, "no resident state: call swe_resident_load first");
+    if (n_steps < 0) return fail(SWE_ERR_INVALID, "n_steps must be >= 0");
+    return enqueue_run_steps(d, d->resident_steps, n_steps, nullptr, false);
+}
+
 int swe_resident_store(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, swe_run_result* result,
                        void* stream) {
     if (!d || !result) return fail(SWE_ERR_INVALID, "null argument");
@@ -1516,7 +1533,7 @@ int swe_resident_store(swe_domain_t d, float* h, float* hu, float* hv, int64_t p
     }
     rc = fold_ledger(d, make_plan(d, d->run_vec, true).blocks, st);
     if (rc) return rc;
-    SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+    SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl, kControlHead, cudaMemcpyDeviceToHost, st));
     SWE_CK(cudaStreamSynchronize(st));
     const Control& c = d->ctl_host[0];
     result->final_time_s = c.t;
@@ -2212,11 +2229,12 @@ int swe_generate_lognormal_field(int32_t rows, int32_t cols, double median, doub
 // A strip owns global rows [row_begin, row_end) and also holds the row below
 // and the row above it when they exist (halo rows, read as ordinary neighbours
 // and never updated).  One step of the whole domain is, per strip: the step
-// kernel over the owned rows (its fold keeps the strip's CFL maximum), the
+// kernel over the owned rows (its warps leave the strip's CFL maximum in the
+// stripes), stripe_fold_kernel (that maximum into the control block), the
 // maximum over strips (NCCL all-reduce, or a kernel when all strips are in one
-// process), plan_kernel (the next dt from that maximum, the same on every
-// strip), and the halo exchange of the new state (each strip's first and last
-// owned rows to its neighbours).
+// process), which the next step of every strip plans from (the same dt on
+// every strip), and the halo exchange of the new state (each strip's first and
+// last owned rows to its neighbours).
 
 }  // extern "C"
 
@@ -2330,7 +2348,7 @@ int strip_finish(swe_domain* d, float* h, float* hu, float* hv, int64_t pitch, i
         const int rc = copy_plane(outs[f], pitch, d->ping[fb][f], d->ppitch, d->dd.rows, d->dd.cols, st);
         if (rc) return rc;
     }
-    SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+    SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl, kControlHead, cudaMemcpyDeviceToHost, st));
     SWE_CK(cudaStreamSynchronize(st));
     const Control& c = d->ctl_host[0];
     r->final_time_s = c.t;
@@ -2535,16 +2553,19 @@ int swe_strips_advance(const swe_domain_t* strips, int32_t n, float* const* h, f
     StripCtls table{};
     table.n = n;
     for (int i = 0; i < n; ++i) table.c[i] = strips[i]->ctl;
-    auto plan_all = [&]() {
+    // The maximum across strips that the next step of every strip plans from:
+    // the start reductions' maxima first, then each step's from its stripes.
+    auto max_all = [&](bool fold) {
+        if (fold)
+            for (int i = 0; i < n; ++i) stripe_fold_kernel<<<1, 32, 0, st>>>(strips[i]->ctl);
         strips_max_kernel<<<1, 32, 0, st>>>(table);
-        for (int i = 0; i < n; ++i) plan_kernel<<<1, 1, 0, st>>>(strips[i]->dd, strips[i]->ctl);
     };
     int rc = SWE_OK;
-    plan_all();
+    max_all(false);
     const int cols = strips[0]->dd.cols;
     for (int k = 0; k < n_steps && !rc; ++k) {
         for (int i = 0; i < n; ++i) strip_step(strips[i], k, st);
-        plan_all();
+        max_all(true);
         const int b = (k + 1) & 1;
         for (int i = 0; i + 1 < n && !rc; ++i) {
             swe_domain* L = strips[i];
@@ -2607,17 +2628,19 @@ int swe_strip_advance_nccl(swe_domain_t d, swe_comm_t comm, int32_t rank_below, 
     // 3. The steps.  Each NCCL call is settled; the group is always closed.
     const int cols = d->dd.cols;
     const HaloRows hr = halo_rows(d);
-    auto plan = [&]() -> int {
+    // The maximum across strips that the next step plans from: the start
+    // reduction's maximum first, then each step's from its stripes.
+    auto max_all = [&](bool fold) -> int {
+        if (fold) stripe_fold_kernel<<<1, 32, 0, st>>>(d->ctl);
         const ncclResult_t e = nccl_settle(api, comm, api->AllReduce(&d->ctl->maxinv, &d->ctl->maxinv, 1, ncclFloat,
                                                                      ncclMax, comm->comm, st));
         if (e != ncclSuccess) return nccl_abort(api, comm, std::string("all-reduce: ") + api->GetErrorString(e));
-        plan_kernel<<<1, 1, 0, st>>>(d->dd, d->ctl);
         return SWE_OK;
     };
-    rc = plan();
+    rc = max_all(false);
     for (int k = 0; k < n_steps && !rc; ++k) {
         strip_step(d, k, st);
-        rc = plan();
+        rc = max_all(true);
         if (rc) break;
         const int b = (k + 1) & 1;
         ncclResult_t first = api->GroupStart();

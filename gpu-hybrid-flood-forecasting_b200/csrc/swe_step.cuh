@@ -6,8 +6,11 @@
 // ghost ring, wall mirroring, hydrostatic reconstruction, HLL x/y fluxes,
 // divergence, rain source, positivity clip, semi-implicit Manning friction,
 // wet/dry masking -- and, in run mode, the CFL inverse-dt reduction of the NEW
-// state (numerics.py:297-309) plus FP64 mass-ledger partials, finished by the
-// last CTA, which also advances the device-resident FP64 clock.
+// state (numerics.py:297-309) plus FP64 mass-ledger sums.  A run step plans
+// itself: each warp reads the run position (FP64 clock, next output) and the
+// previous step's CFL maximum and computes the same dt, one warp per run
+// publishes the advanced position, and each warp ends with an atomic maximum
+// and its own ledger slot, so no warp waits for another.
 //
 // Work decomposition ("column marching"): a warp owns a strip of 32*V columns
 // (V consecutive columns per lane, loaded as float2/float4) and marches up a
@@ -22,6 +25,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "swe_math.cuh"
@@ -58,6 +62,7 @@ struct DomainDev {
     const double* rain_t;  // hyetograph times (s), float64 copies of the float32 table
     const double* rain_r;  // rates (m/s)
     int n_rain;
+    double rain_x0, rain_xn, rain_yn;  // first and last time of the hyetograph, last rate
     double rain_scale;     // multiplies every rate (1 = the hyetograph as given)
     // Rows the step updates and the reductions cover: [upd_lo, upd_hi).  A row
     // strip of a decomposed domain also holds its neighbours' boundary rows
@@ -79,38 +84,78 @@ struct StateOut {
     int64_t pitch;
 };
 
-// Device-resident run control: clock, next dt, output bookkeeping, ledger.
+// Hyetograph segment [x0, x1) with its rates at both ends, kept between steps
+// (lo = -1: none yet).
+struct RainSeg {
+    double x0, y0, x1, y1;
+    double slope;  // (y1 - y0) / (x1 - x0), rounded as np.interp rounds it
+    int lo;
+};
+
+// The run's position at the start of a step.  There is one copy per step
+// parity: step k plans itself from copy k&1, and its lead warp writes copy
+// (k+1)&1, so a step never writes what its own warps read.
+struct alignas(16) RunPos {
+    double t;       // simulated time at the start of the step
+    double target;  // output time `idx` in float64 (valid while idx < n_out)
+    RainSeg rain;   // the segment of the previous step's rain rate
+    int steps;      // steps taken
+    int idx;        // next output index to fill
+    int done;       // nonzero: all outputs written, step cap reached or failure
+    int status;     // 0 ok, else an SWE_ERR_* code
+};
+
+// CFL maxima of the steps: per step parity, kMaxStripes words 128 bytes apart,
+// each the atomic maximum of (steps of the state << 32 | float bits of its
+// largest inverse dt) over the warps that chose it.  The step count in the
+// high word makes a newer step's value beat whatever an older step left, so
+// the words are never cleared during a run.
+constexpr int kMaxStripes = 16;
+constexpr int kStripeWords = 16;
+
+// Device-resident run control: output bookkeeping, ledger, the run position
+// of each step parity and the CFL maxima.  The fields up to `pos` are the
+// host's view, published by the lead warp of every step (and by the run's
+// start reduction).
 struct Control {
-    double t;          // simulated time at the start of the next step
-    double dt;         // dt of the next step (already limited by the output target)
-    StepScalars s;     // float32 scalars of the next step
-    int snap;          // output index written by the next step, -1 if none
-    int reach;         // output time reached by the next step (recorded or not), -1 if none
+    double t;          // simulated time reached
+    double dt;         // dt of the last step taken
     int idx;           // next output index to fill
     int steps;         // steps taken
     int done;          // nonzero: all outputs written, step cap hit or failure
     int status;        // 0 ok, else an SWE_ERR_* code
-    float maxinv;      // max inverse CFL dt of the current state
-    unsigned counter;  // last-CTA ticket
+    float maxinv;      // max inverse CFL dt: of the initial state, or across the strips of a domain
+    unsigned counter;  // last-CTA ticket of the start reduction
     int n_out, max_steps;
-    double t_start;               // clock value set by the init reduction
+    double t_start;               // clock value set by the start reduction
     const float* times;           // device copy of the float32 output times
     const double* times64;        // float64 targets instead of `times` (advance_to), or null
     unsigned* done_counter;       // incremented once when this run finishes (ensembles), or null
-    double* dt_log;               // dt of every planned step (index = step number), or null
+    double* dt_log;               // dt of every step (index = step number), or null
     float* out_h;                 // n_out x rows x cols snapshots (may be null)
     float* out_hu;
     float* out_hv;
     int64_t out_plane;            // rows * cols
     double ledger[6];             // volume0, volume, rain_in, outflow, clip_gain, mask_loss
-    int defer_plan;               // 1: the fold leaves maxinv (NaN as +inf) for plan_kernel to use
-    int rain_seg;                 // hyetograph segment of the last planned step (a search hint)
-    unsigned max_bits;            // the step's CFL maximum as float bits (atomicMax), 0 between steps
+    int defer_plan;               // 1: steps plan from `maxinv` (set across strips), not from the stripes
+    RunPos pos[2];
+    alignas(128) unsigned long long maxk[2][kMaxStripes * kStripeWords];
 };
+
+// Bytes of the control block the host reads back (everything before the maxima).
+constexpr size_t kControlHead = offsetof(Control, maxk);
 
 struct Partial {
     float maxinv;
     double vol, rain, outflow, clip, mask;
+};
+
+// A warp's ledger slot of a run: its cells' volume after the last step, and
+// the rain, outflow, clip and mask terms summed over the run's steps.  The
+// first four words are read back at the start of each step (two 16-byte
+// copies), so the slot is 16-byte aligned.
+struct alignas(16) LedgerSlot {
+    double rain, outflow, clip, mask, vol, pad;
 };
 
 // ---------------------------------------------------------------------------
@@ -271,39 +316,33 @@ __device__ __forceinline__ FaceFlux face_flux(const Cell& lo, const Cell& hi, co
 // ---------------------------------------------------------------------------
 // np.interp(t, times, rates, left=default, right=default) in float64 with
 // separately rounded operations (shallow_water_2d.py:254-264).
-// `seg` (may be null) caches the segment of the previous call: a run's clock only
-// advances, so the segment is usually the same or the next one, and checking
-// those two replaces the binary search's chain of dependent loads.  A cached
-// segment is used only when it contains t (rain_t[lo] <= t < rain_t[lo + 1]),
-// where it is the one the search finds.
-__device__ inline double rain_rate_unscaled(const DomainDev& d, double t, int* seg = nullptr) {
+// The segment containing t comes from `sg` when the cached one contains it
+// (x0 <= t < x1): a run's clock only advances, so a step's segment is nearly
+// always the previous step's, and the cache then replaces every load of the
+// table.  Otherwise it is found by binary search and `sg` is updated.  For a
+// sorted table the non-empty segment containing t is unique, so both ways
+// give the same segment and the same value.
+__device__ inline double rain_rate_unscaled(const DomainDev& d, double t, RainSeg& sg) {
     const int n = d.n_rain;
     if (n <= 0) return d.default_rain;
-    const double x0 = d.rain_t[0], xn = d.rain_t[n - 1];
     if (t != t) return t;
-    if (t < x0 || t > xn) return d.default_rain;
-    if (n == 1 || t == xn) return d.rain_r[n - 1];
-    int lo = -1;
-    if (seg) {
-        for (int cand = *seg; cand <= *seg + 1; ++cand)
-            if (cand >= 0 && cand < n - 1 && d.rain_t[cand] <= t && t < d.rain_t[cand + 1]) {
-                lo = cand;
-                break;
-            }
-    }
-    if (lo < 0) {
-        lo = 0;
-        int hi = n - 1;
+    if (t < d.rain_x0 || t > d.rain_xn) return d.default_rain;
+    if (n == 1 || t == d.rain_xn) return d.rain_yn;
+    if (!(sg.lo >= 0 && sg.x0 <= t && t < sg.x1)) {
+        int lo = 0, hi = n - 1;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
             if (d.rain_t[mid] <= t) lo = mid; else hi = mid;
         }
+        sg.lo = lo;
+        sg.x0 = d.rain_t[lo];
+        sg.y0 = d.rain_r[lo];
+        sg.x1 = d.rain_t[lo + 1];
+        sg.y1 = d.rain_r[lo + 1];
+        sg.slope = __ddiv_rn(__dsub_rn(sg.y1, sg.y0), __dsub_rn(sg.x1, sg.x0));
     }
-    if (seg) *seg = lo;
-    const double xj = d.rain_t[lo], yj = d.rain_r[lo];
+    const double xj = sg.x0, yj = sg.y0, xj1 = sg.x1, yj1 = sg.y1, slope = sg.slope;
     if (t == xj) return yj;
-    const double xj1 = d.rain_t[lo + 1], yj1 = d.rain_r[lo + 1];
-    const double slope = __ddiv_rn(__dsub_rn(yj1, yj), __dsub_rn(xj1, xj));
     double v = __dadd_rn(__dmul_rn(slope, __dsub_rn(t, xj)), yj);
     if (v != v) {
         v = __dadd_rn(__dmul_rn(slope, __dsub_rn(t, xj1)), yj1);
@@ -312,15 +351,11 @@ __device__ inline double rain_rate_unscaled(const DomainDev& d, double t, int* s
     return v;
 }
 
-__device__ inline double rain_rate(const DomainDev& d, double t, int* seg = nullptr) {
-    return __dmul_rn(d.rain_scale, rain_rate_unscaled(d, t, seg));
-}
-
 // Float32 scalars of a step of length dt starting at t.
-__device__ inline StepScalars step_scalars(const DomainDev& d, double dt, double t, int* seg = nullptr) {
+__device__ inline StepScalars step_scalars(const DomainDev& d, double dt, double t, RainSeg& sg) {
     StepScalars s;
     s.dt = __double2float_rn(dt);
-    s.dt_rain = __double2float_rn(__dmul_rn(dt, rain_rate(d, t, seg)));
+    s.dt_rain = __double2float_rn(__dmul_rn(dt, __dmul_rn(d.rain_scale, rain_rate_unscaled(d, t, sg))));
     s.dt_g = __double2float_rn(__dmul_rn(dt, d.g));
     return s;
 }
@@ -335,31 +370,98 @@ __device__ inline double cfl_dt_from(const DomainDev& d, float maxinv) {
     return d.max_dt;
 }
 
-// Plan the next step from the clock and the CFL maximum (run loop of
-// shallow_water_2d.py:402-412): dt = min(cfl_dt, target - t), record when the
-// new time reaches target - 1e-7, stop when all outputs are written or the step
-// cap is reached.
-__device__ inline void plan_next(const DomainDev& d, Control& c) {
-    c.snap = -1;
-    c.reach = -1;
-    if (c.idx >= c.n_out || c.steps >= c.max_steps) {
-        c.done = 1;
-        return;
+// A step's plan, computed from its run position and the CFL maximum of the
+// state it starts from (run loop of shallow_water_2d.py:402-412): dt =
+// min(cfl_dt, target - t), the output is recorded when the new time reaches
+// target - 1e-7, the run stops when all outputs are written, the step cap is
+// reached or the maximum is not finite.
+struct StepPlan {
+    StepScalars s;
+    double dt;
+    RainSeg rain;  // the segment of this step's rain rate
+    int go;        // 1: the step runs
+    int status;    // the run's status (SWE_ERR_NONFINITE when it stops on a non-finite maximum)
+    int reach;     // output index the new time reaches, -1 if none
+    int snap;      // output index written by the step (reach, when outputs are recorded), -1 if none
+};
+
+// Everything a warp reads to plan a step: the run position of the step's
+// parity, this lane's CFL maximum word, and the run's constants.
+struct PlanInputs {
+    RunPos pos;
+    unsigned long long w;   // maximum word `lane` of the parity (lanes < kMaxStripes)
+    float gmax;             // the maximum across strips (row strips of a decomposed domain)
+    int defer, n_out, max_steps;
+    const float* out_h;
+    double* dt_log;
+    unsigned* done_counter;
+};
+
+// Issues the loads of a step's plan (every lane).  They are plain loads: the
+// previous step's writes are visible after griddepcontrol.wait, which the
+// kernel has passed, and a load that every warp of an SM makes is then merged
+// in the SM's L1 instead of reaching one L2 slice from every warp of the grid.
+// The values are consumed later (plan_step), so the caller can start other
+// loads while these are in flight.
+__device__ __forceinline__ PlanInputs plan_fetch(const Control* c, int par) {
+    const int lane = threadIdx.x & 31;
+    PlanInputs in;
+    in.pos = c->pos[par];
+    in.w = lane < kMaxStripes ? c->maxk[par][lane * kStripeWords] : 0ull;
+    in.gmax = c->maxinv;
+    in.defer = c->defer_plan;
+    in.n_out = c->n_out;
+    in.max_steps = c->max_steps;
+    in.out_h = c->out_h;
+    in.dt_log = c->dt_log;
+    in.done_counter = c->done_counter;
+    return in;
+}
+
+// The CFL maximum of the state with `steps` steps taken, from the words of
+// one parity (word `lane` in `w` on lanes < kMaxStripes) that carry that step
+// count; NaN when none does, which stops the run as non-finite.  Every lane
+// of the warp returns it.
+__device__ __forceinline__ float words_maxinv(unsigned long long w, int steps) {
+    const bool mine = (threadIdx.x & 31) < kMaxStripes && (int)(w >> 32) == steps;
+    const unsigned m = __reduce_max_sync(0xffffffffu, mine ? (unsigned)w : 0u);
+    const bool found = __any_sync(0xffffffffu, mine);
+    return found ? __uint_as_float(m) : __int_as_float(0x7fffffff);
+}
+
+// The plan from the fetched inputs (every lane, the same values): the maximum
+// from the words, or, for a strip of a decomposed domain, across strips.
+__device__ inline StepPlan plan_step(const DomainDev& d, const PlanInputs& in) {
+    const RunPos& pos = in.pos;
+    const float wmax = words_maxinv(in.w, pos.steps);
+    const float maxinv = in.defer ? in.gmax : wmax;
+    StepPlan p;
+    p.go = 0;
+    p.status = pos.status;
+    p.reach = p.snap = -1;
+    p.dt = 0.0;
+    p.s = StepScalars{0.f, 0.f, 0.f};
+    p.rain = pos.rain;
+    if (pos.done || pos.idx >= in.n_out || pos.steps >= in.max_steps) return p;
+    if (!(maxinv == maxinv) || isinf(maxinv)) {
+        p.status = 4;  // SWE_ERR_NONFINITE
+        return p;
     }
-    if (!(c.maxinv == c.maxinv) || isinf(c.maxinv)) {
-        c.done = 1;
-        c.status = 4;  // SWE_ERR_NONFINITE
-        return;
-    }
-    const double target = c.times64 ? c.times64[c.idx] : (double)c.times[c.idx];
-    double dt = cfl_dt_from(d, c.maxinv);
-    const double remain = __dsub_rn(target, c.t);
+    double dt = cfl_dt_from(d, maxinv);
+    const double remain = __dsub_rn(pos.target, pos.t);
     if (remain < dt) dt = remain;
-    c.dt = dt;
-    c.s = step_scalars(d, dt, c.t, &c.rain_seg);
-    c.reach = (__dadd_rn(c.t, dt) >= __dsub_rn(target, 1.0e-7)) ? c.idx : -1;
+    p.dt = dt;
+    p.s = step_scalars(d, dt, pos.t, p.rain);
+    p.reach = (__dadd_rn(pos.t, dt) >= __dsub_rn(pos.target, 1.0e-7)) ? pos.idx : -1;
     // Without output buffers (advance, advance_to) nothing is recorded.
-    c.snap = c.out_h ? c.reach : -1;
+    p.snap = in.out_h ? p.reach : -1;
+    p.go = 1;
+    return p;
+}
+
+// Float64 output time i of a run.
+__device__ __forceinline__ double output_time(const Control* c, int i) {
+    return c->times64 ? c->times64[i] : (double)c->times[i];
 }
 
 // Programmatic dependent launch: a step kernel launched with the programmatic
@@ -412,16 +514,6 @@ struct StepAccum {
     }
 };
 
-// Reduce per-thread accumulators over the CTA in a fixed order, write the CTA
-// partial, and let the last CTA to finish fold all partials (again in a fixed
-// order, so the ledger is bitwise reproducible) and advance the control block.
-// Bookkeeping once the next step is planned: its dt in the log, the ensemble's
-// completion counter.
-__device__ __forceinline__ void after_plan(Control& c) {
-    if (!c.done && c.dt_log) c.dt_log[c.steps] = c.dt;  // steps < max_steps while not done
-    if (c.done && c.done_counter) atomicAdd(c.done_counter, 1u);
-}
-
 // CTA-wide reduction of a thread's accumulators (fixed order) into the CTA's
 // totals, valid on thread 0.
 template <int THREADS>
@@ -460,71 +552,20 @@ __device__ __forceinline__ Partial cta_reduce(Accum acc) {
     return p;
 }
 
-// End of a step (or of the reduction that starts a run) for one CTA.
+// End of the reduction that starts a run (reduce_kernel): the CTA partials are
+// folded by the last CTA to arrive, in a fixed order, into the initial volume
+// and CFL maximum, and the run's first position is set: clock at t_start,
+// output 0 taken as the initial state, the first target loaded, the maximum
+// stored for step 0 (step count 0 in the high word of stripe 0).
 //
-// Step: the CTA's ledger terms go into its own slot of `parts` (the volume
-// replaced, the other terms added: each slot sums its cells over the whole run
-// in a fixed order, and ledger_fold_kernel adds the slots when the run's
-// results are read); its CFL maximum goes into the control block by an
-// atomic maximum of the float bits (a NaN volume, i.e. a non-finite state in
-// the CTA, counts as NaN, which beats every finite bit pattern); the last CTA
-// of the domain to arrive takes the maximum, advances the clock and plans the
-// next step.  The serial tail of a step is thus one ticket, one exchange and
-// the plan: the ledger sums, which no step needs, are off that path.
-//
-// Start of a run (init): the reduction's CTA partials are folded by the last
-// CTA in a fixed order into volume0 and the first CFL maximum.
-//
-// PER: partials a thread of the last CTA loads before folding them in init.
+// PER: partials a thread of the last CTA loads before folding them.
 template <int THREADS, int PER = 8>
-__device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts, Accum acc,
-                                bool init, int part = -1, int nparts = -1) {
-    // One slot per CTA of this domain: by default the launch's CTAs; the
-    // ensemble kernel passes the CTA's slot within its member instead.
-    if (part < 0) {
-        part = blockIdx.x;
-        nparts = gridDim.x;
-    }
+__device__ void finish_start(const DomainDev& d, Control* ctl, Partial* parts, Accum acc) {
+    const int nparts = gridDim.x;
     __shared__ bool s_last;
     const Partial p = cta_reduce<THREADS>(acc);
-    if (!init) {
-        if (threadIdx.x != 0) return;
-        Partial& q = parts[part];
-        q.vol = p.vol;
-        q.rain += p.rain;
-        q.outflow += p.outflow;
-        q.clip += p.clip;
-        q.mask += p.mask;
-        const unsigned bits =
-            (p.vol == p.vol) ? (__float_as_uint(p.maxinv) & 0x7fffffffu) : 0x7fc00000u;
-        atomicMax(&ctl->max_bits, bits);
-        __threadfence();
-        const unsigned ticket = atomicAdd(&ctl->counter, 1u);
-        if (ticket != (unsigned)nparts - 1) return;
-        __threadfence();
-        const float mx = __uint_as_float(atomicExch(&ctl->max_bits, 0u));
-        Control c = *ctl;
-        c.t = __dadd_rn(c.t, c.dt);
-        c.steps += 1;
-        if (c.reach >= 0) c.idx = c.reach + 1;
-        c.maxinv = mx;
-        c.counter = 0;
-        c.max_bits = 0;
-        if (c.defer_plan) {
-            // A row strip: the CFL maximum of the whole domain is formed across the
-            // strips first (NaN kept as +inf so that a maximum carries it), then
-            // plan_kernel plans the step.
-            if (!(mx == mx)) c.maxinv = INFINITY;
-        } else {
-            plan_next(d, c);
-            after_plan(c);
-        }
-        *ctl = c;
-        __threadfence();
-        return;
-    }
     if (threadIdx.x == 0) {
-        parts[part] = p;
+        parts[blockIdx.x] = p;
         __threadfence();
         const unsigned ticket = atomicAdd(&ctl->counter, 1u);
         s_last = (ticket == (unsigned)nparts - 1);
@@ -546,18 +587,13 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
             if (b < nparts) {
                 buf[j].maxinv = __ldcg(&parts[b].maxinv);
                 buf[j].vol = __ldcg(&parts[b].vol);
-                buf[j].rain = __ldcg(&parts[b].rain);
-                buf[j].outflow = __ldcg(&parts[b].outflow);
-                buf[j].clip = __ldcg(&parts[b].clip);
-                buf[j].mask = __ldcg(&parts[b].mask);
             }
         }
 #pragma unroll
         for (int j = 0; j < kPer; ++j) {
             if (base + j * THREADS < nparts) {
                 a.maxinv = nan_max(a.maxinv, buf[j].maxinv);
-                a.vol += buf[j].vol; a.rain += buf[j].rain; a.outflow += buf[j].outflow;
-                a.clip += buf[j].clip; a.mask += buf[j].mask;
+                a.vol += buf[j].vol;
             }
         }
     }
@@ -565,42 +601,149 @@ __device__ void finish_run_step(const DomainDev& d, Control* ctl, Partial* parts
     if (threadIdx.x != 0) return;
     float mx = t.maxinv;
     // A NaN volume means a non-finite state somewhere: report it as a NaN CFL
-    // maximum, the form plan_next tests.
+    // maximum, the form plan_step tests.
     if (!(t.vol == t.vol)) mx = __int_as_float(0x7fffffff);
-    Control c = *ctl;
     const double area = d.dx * d.dy;
-    c.t = c.t_start;
-    c.idx = 1;
-    c.steps = 0;
-    c.done = 0;
-    c.status = 0;
-    c.ledger[0] = t.vol * area;
-    c.ledger[1] = t.vol * area;
-    c.ledger[2] = c.ledger[3] = c.ledger[4] = c.ledger[5] = 0.0;
-    c.maxinv = mx;
-    c.counter = 0;
-    c.max_bits = 0;
-    if (c.defer_plan) {
-        if (!(mx == mx)) c.maxinv = INFINITY;
-    } else {
-        plan_next(d, c);
-        after_plan(c);
-    }
-    *ctl = c;
+    const int n_out = ctl->n_out;
+    RunPos p0;
+    p0.t = ctl->t_start;
+    p0.target = n_out > 1 ? output_time(ctl, 1) : 0.0;
+    p0.rain = RainSeg{0.0, 0.0, 0.0, 0.0, 0.0, -1};
+    p0.steps = 0;
+    p0.idx = 1;
+    p0.done = (1 >= n_out || ctl->max_steps <= 0) ? 1 : 0;
+    p0.status = 0;
+    ctl->pos[0] = p0;
+    ctl->t = p0.t;
+    ctl->dt = 0.0;
+    ctl->idx = 1;
+    ctl->steps = 0;
+    ctl->done = p0.done;
+    ctl->status = 0;
+    ctl->ledger[0] = t.vol * area;
+    ctl->ledger[1] = t.vol * area;
+    ctl->ledger[2] = ctl->ledger[3] = ctl->ledger[4] = ctl->ledger[5] = 0.0;
+    // A row strip plans from the maximum across strips: NaN is kept as +inf
+    // there, so that a maximum carries it.
+    ctl->maxinv = (ctl->defer_plan && !(mx == mx)) ? INFINITY : mx;
+    ctl->maxk[0][0] = (unsigned long long)(__float_as_uint(mx) & 0x7fffffffu);
+    ctl->counter = 0;
+    if (p0.done && ctl->done_counter) atomicAdd(ctl->done_counter, 1u);
     __threadfence();
 }
 
-// The run's ledger from the step CTAs' slots (one CTA, fixed order): the stored
+// The CFL maximum of the state with `steps` steps taken, from the words of
+// parity `par` (one load per lane).
+__device__ __forceinline__ float stripes_maxinv(const Control* c, int par, int steps) {
+    const int lane = threadIdx.x & 31;
+    return words_maxinv(lane < kMaxStripes ? c->maxk[par][lane * kStripeWords] : 0ull, steps);
+}
+
+// Start of a step in a warp, with nothing to overlap: its run position
+// (parity `par`) and its plan, the same on every lane.
+__device__ __forceinline__ StepPlan warp_plan(const DomainDev& d, const Control* c, int par, PlanInputs& in) {
+    in = plan_fetch(c, par);
+    return plan_step(d, in);
+}
+
+// The lead warp of a run (one per run and step) advances the run position into
+// the other parity's copy and publishes it: clock, step count, next output,
+// completion (set as soon as the last output is written or the step cap is
+// reached, so the host sees it after the step that ends the run), the dt log
+// and an ensemble's completion counter.  A finished run's position is copied
+// forward unchanged, so every later step of either parity sees it finished.
+// Stores only, except the time of the next output when the step records one.
+__device__ __forceinline__ void lead_advance(Control* c, int par, const PlanInputs& in, const StepPlan& p) {
+    if ((threadIdx.x & 31) != 0) return;
+    const RunPos& pos = in.pos;
+    RunPos q = pos;
+    int newly_done = 0;
+    if (!pos.done) {
+        if (!p.go) {
+            q.done = 1;
+            q.status = p.status;
+            newly_done = 1;
+        } else {
+            q.t = __dadd_rn(pos.t, p.dt);
+            q.steps = pos.steps + 1;
+            q.rain = p.rain;
+            if (p.reach >= 0) {
+                q.idx = p.reach + 1;
+                if (q.idx < in.n_out) q.target = output_time(c, q.idx);
+            }
+            q.done = (q.idx >= in.n_out || q.steps >= in.max_steps) ? 1 : 0;
+            newly_done = q.done;
+            if (in.dt_log) in.dt_log[pos.steps] = p.dt;  // steps < max_steps while not done
+            c->dt = p.dt;
+        }
+    }
+    c->pos[par ^ 1] = q;
+    c->t = q.t;
+    c->idx = q.idx;
+    c->steps = q.steps;
+    c->done = q.done;
+    c->status = q.status;
+    if (newly_done && in.done_counter) atomicAdd(in.done_counter, 1u);
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned).
+__device__ __forceinline__ void cp_async_16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+
+// Starts the copy of the warp's ledger slot (rain, outflow, clip, mask summed
+// so far) into `old` (4 doubles of the warp's shared memory, 16-byte aligned):
+// lanes 0 and 1 copy 16 bytes each.  The caller commits the group.
+__device__ __forceinline__ void ledger_prefetch(const LedgerSlot* slot, double* old) {
+    const int lane = threadIdx.x & 31;
+    if (lane < 2) cp_async_16(old + 2 * lane, &slot->rain + 2 * lane);
+}
+
+// End of a step in a warp, once the prefetched slot has landed: the warp's
+// ledger terms (fixed-order butterfly sums) go into its slot, the volume
+// replaced and the other terms added to the run's sums, and its CFL maximum
+// into stripe `stripe` of the next parity, tagged with the step count of the
+// new state.  A NaN volume (a non-finite state in the warp's cells) counts as
+// a NaN maximum, which beats every finite bit pattern.  Nothing here waits:
+// the stores and the atomic maximum are complete when the grid is.
+__device__ __forceinline__ void warp_end_step(Control* c, LedgerSlot* slot, const double* old, int par, int steps,
+                                              int stripe, Accum a) {
+    const double vol = warp_sum(a.vol);
+    const double rain = warp_sum(a.rain);
+    const double outflow = warp_sum(a.outflow);
+    const double clip = warp_sum(a.clip);
+    const double mask = warp_sum(a.mask);
+    unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(a.maxinv) & 0x7fffffffu);
+    if (!(vol == vol)) m = 0x7fc00000u;
+    if ((threadIdx.x & 31) != 0) return;
+    slot->vol = vol;
+    slot->rain = old[0] + rain;
+    slot->outflow = old[1] + outflow;
+    slot->clip = old[2] + clip;
+    slot->mask = old[3] + mask;
+    atomicMax(&c->maxk[par ^ 1][stripe * kStripeWords], ((unsigned long long)(steps + 1) << 32) | m);
+}
+
+// The run's ledger from the warps' slots (one CTA, fixed order): the stored
 // volume of the last step and the rain, outflow, clip and mask terms summed over
 // the run.  With no step taken the volume stays the initial one.
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) ledger_fold_kernel(const DomainDev d, Control* ctl, const Partial* parts,
+__global__ void __launch_bounds__(THREADS) ledger_fold_kernel(const DomainDev d, Control* ctl, const LedgerSlot* slots,
                                                              int nslots) {
     Accum a;
     a.zero();
     for (int b = threadIdx.x; b < nslots; b += THREADS) {
-        a.vol += parts[b].vol; a.rain += parts[b].rain; a.outflow += parts[b].outflow;
-        a.clip += parts[b].clip; a.mask += parts[b].mask;
+        a.vol += slots[b].vol; a.rain += slots[b].rain; a.outflow += slots[b].outflow;
+        a.clip += slots[b].clip; a.mask += slots[b].mask;
     }
     const Partial t = cta_reduce<THREADS>(a);
     if (threadIdx.x != 0) return;
@@ -612,13 +755,13 @@ __global__ void __launch_bounds__(THREADS) ledger_fold_kernel(const DomainDev d,
     ctl->ledger[5] = t.mask * area;
 }
 
-// Plans the next step of a row strip from the domain-wide CFL maximum now in
-// ctl->maxinv (single thread).
-__global__ void plan_kernel(const DomainDev d, Control* ctl) {
-    Control c = *ctl;
-    plan_next(d, c);
-    after_plan(c);
-    *ctl = c;
+// A row strip's CFL maximum after its step, from the stripes of the step's
+// parity, into ctl->maxinv (NaN as +inf), for the maximum across strips that
+// the next step plans from.  One warp.
+__global__ void stripe_fold_kernel(Control* ctl) {
+    const int steps = __ldcg(&ctl->steps);
+    const float m = stripes_maxinv(ctl, steps & 1, steps);
+    if (threadIdx.x == 0) ctl->maxinv = (m == m) ? m : INFINITY;
 }
 
 // ---------------------------------------------------------------------------
@@ -630,7 +773,8 @@ struct StepLaunch {
     StateOut out;
     StepScalars s;     // used when ctl == nullptr (plain step)
     Control* ctl;      // run mode when non-null
-    Partial* parts;
+    LedgerSlot* slots; // run mode: one ledger slot per warp of the launch
+    int par;           // run mode: parity of the step (k & 1 for the run's step k)
     int nstrips;       // ceil(cols / (32 V))
     int rows_per_warp;
 };
@@ -653,23 +797,34 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
     __shared__ float s_left[NW][3][kBatch];
     __shared__ float s_right[NW][7][kBatch];
 
+    __shared__ alignas(16) double s_old[NW][4];  // the warp's ledger slot as the step found it
+
     pdl_enter();
     const DomainDev& d = p.d;
     const Consts& k = d.k;
     constexpr bool run = RUN;
-    StepScalars s = p.s;
-    int snap = -1;
-    double dtd = 0.0;
-    if constexpr (RUN) {
-        const Control* c = p.ctl;
-        if (*((volatile const int*)&c->done)) return;  // uniform early exit of the whole grid
-        s = c->s;
-        snap = c->snap;
-        dtd = c->dt;
-    }
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int gw = blockIdx.x * NW + wib;
+    StepScalars s = p.s;
+    int snap = -1;
+    double dtd = 0.0;
+    int steps0 = 0;
+    if constexpr (RUN) {
+        ledger_prefetch(&p.slots[gw], s_old[wib]);
+        cp_async_commit();
+        PlanInputs in;
+        const StepPlan pl = warp_plan(d, p.ctl, p.par, in);
+        if (blockIdx.x == 0 && wib == 0) lead_advance(p.ctl, p.par, in, pl);
+        if (!pl.go) {  // uniform over the grid: the run has ended
+            cp_async_wait<0>();
+            return;
+        }
+        s = pl.s;
+        snap = pl.snap;
+        dtd = pl.dt;
+        steps0 = in.pos.steps;
+    }
     const int strip = gw % p.nstrips;
     const int chunk = gw / p.nstrips;
     const int r0 = d.upd_lo + chunk * p.rows_per_warp;
@@ -900,7 +1055,9 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
         a.outflow = acc.outflow;
         a.clip = acc.clip;
         a.mask = acc.mask;
-        finish_run_step<THREADS>(d, p.ctl, p.parts, a, false);
+        cp_async_wait<0>();
+        __syncwarp();
+        warp_end_step(p.ctl, &p.slots[gw], s_old[wib], p.par, steps0, gw % kMaxStripes, a);
     }
 }
 
@@ -927,7 +1084,7 @@ __global__ void __launch_bounds__(THREADS) reduce_kernel(const DomainDev d, cons
         acc.maxinv = nan_max(acc.maxinv, act ? inv : 0.0f);
         if (act) acc.vol += (double)h;
     }
-    finish_run_step<THREADS>(d, ctl, parts, acc, true);
+    finish_start<THREADS>(d, ctl, parts, acc);
 }
 
 }  // namespace swe

@@ -30,11 +30,6 @@ __device__ __forceinline__ KScalar make_kscalar(const Consts& k) {
 
 constexpr int kRing = 4;  // rows in flight per warp (a power of two)
 
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 #ifndef SWE_PAIR_MINBLOCKS
 #define SWE_PAIR_MINBLOCKS 4
@@ -47,6 +42,7 @@ struct WarpSmem {
     float right[7][kWarp];     // the cell right of the strip, per batch row
     float2 ring[kRing][5][kWarp];  // [slot][field][lane]
     double led[5][kWarp];      // float64 ledger sums per lane (vol, rain, clip, mask, outflow)
+    alignas(16) double old[4]; // the warp's ledger slot as the step found it (run mode)
 };
 
 __device__ __forceinline__ void cp_async_8z(void* dst, const void* src, int src_bytes) {
@@ -55,6 +51,15 @@ __device__ __forceinline__ void cp_async_8z(void* dst, const void* src, int src_
                  "l"(src), "r"(src_bytes)
                  : "memory");
 }
+
+// What a march needs from its step's plan: the float32 scalars, the snapshot
+// index, the float64 dt and whether the step runs at all.
+struct MarchPlan {
+    StepScalars s;
+    int snap;
+    double dtd;
+    int go;
+};
 
 // Ledger accumulation (float partials of diagnostics, not step arithmetic): packed FMA in both policies.
 __device__ __forceinline__ float2 lfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
@@ -68,11 +73,10 @@ __device__ __forceinline__ float2 lfma(float2 a, float2 b, float2 c) { return __
 // ring copies by their source size (zero bytes past the chunk or the right
 // edge).  The ledger terms accumulate as float partials over at most one
 // 32-row batch and are folded into the float64 accumulators per batch.
-template <class M, bool RUN, bool MASKED>
-__device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& in,
-                                            const StateOut& out, const StepScalars& s, int snap,
-                                            double dtd, const Control* ctl, int r0, int r1,
-                                            int x0w, WarpSmem& sm, StepAccum& acc) {
+template <class M, bool RUN, bool MASKED, class PlanFn>
+__device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& in,
+                                            const StateOut& out, PlanFn&& plan_fn, const Control* ctl,
+                                            int r0, int r1, int x0w, WarpSmem& sm, StepAccum& acc) {
     constexpr int kBatch = kWarp;
     using A = P<M>;
     const Consts& k = d.k;
@@ -84,10 +88,13 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
     const float2 vmask = f2(valid.x ? 1.f : 0.f, valid.y ? 1.f : 0.f);
     // The component holding the last column: its right x-face is the east boundary.
     const float2 emask = f2(c0 == d.cols - 1 ? 1.f : 0.f, c0 + 1 == d.cols - 1 ? 1.f : 0.f);
-    const float2 dt2 = splat(s.dt), dtr2 = splat(s.dt_rain), dtg2 = splat(s.dt_g);
+    // The step's dt and everything made from it are known once the plan is
+    // (after the march's first loads are in flight).
+    float2 dt2, dtr2, dtg2, ndtdx2, ndtdy2;
+    int snap = -1;
+    double dtd = 0.0;
     const float2 dx2 = splat(k.dx), dy2 = splat(k.dy);
     const float rdx = 1.0f / k.dx, rdy = 1.0f / k.dy;
-    const float2 ndtdx2 = splat(-s.dt * rdx), ndtdy2 = splat(-s.dt * rdy);
     const float2 rdx2 = splat(rdx), rdy2 = splat(rdy);
     const float2 nexpo2 = splat(-k.expo);
     const int nq = r1 - r0 + 2;  // rows r0-1 .. r1 pass through the ring
@@ -375,8 +382,23 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
         if (r + 1 < r1) consume(r + 3 - r0, cur);
     };
     // The first batch's strip edges are loaded before the ring's first rows are
-    // waited for, so that the two latencies of the march's start overlap.
+    // waited for, and the step is planned while the ring's rows are in flight,
+    // so that the latencies of the march's start overlap.
     batch(r0);
+    {
+        const MarchPlan mp = plan_fn();
+        if (!mp.go) {
+            cp_async_wait<0>();
+            return false;
+        }
+        dt2 = splat(mp.s.dt);
+        dtr2 = splat(mp.s.dt_rain);
+        dtg2 = splat(mp.s.dt_g);
+        ndtdx2 = splat(-mp.s.dt * rdx);
+        ndtdy2 = splat(-mp.s.dt * rdy);
+        snap = mp.snap;
+        dtd = mp.dtd;
+    }
     consume(0, R1);  // row r0-1
     consume(1, R0);  // row r0
     {
@@ -410,6 +432,7 @@ __device__ __forceinline__ void march_pair(const DomainDev& d, const StateView& 
         if (!MASKED && d.mult == nullptr) acc.rain_cells += (unsigned)((valid.x ? 1 : 0) + (valid.y ? 1 : 0)) * (unsigned)(r1 - r0);
     }
     cp_async_wait<0>();  // nothing may land after the warp is done
+    return true;
 }
 
 template <class M, int THREADS, bool RUN, bool MASKED>
@@ -418,16 +441,6 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
     __shared__ WarpSmem s_warp[NW];
     pdl_enter();
     const DomainDev& d = p.d;
-    StepScalars s = p.s;
-    int snap = -1;
-    double dtd = 0.0;
-    if constexpr (RUN) {
-        const Control* c = p.ctl;
-        if (*((volatile const int*)&c->done)) return;  // uniform early exit of the whole grid
-        s = c->s;
-        snap = c->snap;
-        dtd = c->dt;
-    }
     const int wib = threadIdx.x >> 5;
     const int gw = blockIdx.x * NW + wib;
     const int strip = gw % p.nstrips;
@@ -436,18 +449,40 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
     const int r1 = min(r0 + p.rows_per_warp, d.upd_hi);
     StepAccum acc;
     acc.zero();
-    if (r0 < d.upd_hi)
-        march_pair<M, RUN, MASKED>(d, p.in, p.out, s, snap, dtd, p.ctl, r0, r1, strip * kWarp * 2,
-                                  s_warp[wib], acc);
     if constexpr (RUN) {
+        // The slot copy and the plan's loads are in flight while the march
+        // starts its own; the plan is made once those are issued.
+        ledger_prefetch(&p.slots[gw], s_warp[wib].old);
+        cp_async_commit();
+        const PlanInputs in = plan_fetch(p.ctl, p.par);
+        StepPlan pl;
+        auto plan_fn = [&]() -> MarchPlan {
+            pl = plan_step(d, in);
+            if (blockIdx.x == 0 && wib == 0) lead_advance(p.ctl, p.par, in, pl);
+            return MarchPlan{pl.s, pl.snap, pl.dt, pl.go};
+        };
+        const bool went = r0 < d.upd_hi
+                              ? march_pair<M, true, MASKED>(d, p.in, p.out, plan_fn, p.ctl, r0, r1, strip * kWarp * 2,
+                                                            s_warp[wib], acc)
+                              : plan_fn().go != 0;
+        if (!went) {  // uniform over the grid: the run has ended
+            cp_async_wait<0>();
+            return;
+        }
         Accum a;
         a.maxinv = acc.maxinv;
         a.vol = acc.vol;
-        a.rain = acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
+        a.rain = acc.rain + (double)acc.rain_cells * (double)pl.s.dt_rain;
         a.outflow = acc.outflow;
         a.clip = acc.clip;
         a.mask = acc.mask;
-        finish_run_step<THREADS>(d, p.ctl, p.parts, a, false);
+        cp_async_wait<0>();
+        __syncwarp();
+        warp_end_step(p.ctl, &p.slots[gw], s_warp[wib].old, p.par, in.pos.steps, gw % kMaxStripes, a);
+    } else {
+        if (r0 < d.upd_hi)
+            march_pair<M, false, MASKED>(d, p.in, p.out, [&]() { return MarchPlan{p.s, -1, 0.0, 1}; }, nullptr, r0,
+                                         r1, strip * kWarp * 2, s_warp[wib], acc);
     }
 }
 
@@ -458,19 +493,62 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
 // Each member is a complete domain (its own static planes, ping-pong state,
 // run control with float64 clock, CFL dt and mass ledger).  The launch's CTAs
 // are persistent: CTA b takes work items b, b + gridDim.x, ...; an item is one
-// CTA's worth of warps of one member (item.y = its slot among the member's
-// `ncta` slots).  After its march the CTA folds into that member's partials and
-// the member's last slot advances the member's clock and plans its next dt, so
-// members step with their own CFL dt and finish independently (a finished
-// member's items return at once).
+// CTA's worth of warps of one member (its slot among the member's `ncta`
+// slots).  Every warp plans its member's step from the member's run position
+// and CFL maximum, so members step with their own CFL dt and finish
+// independently (a finished member's items return at once); the warps of
+// slot 0 lead the member's run position.
 struct MemberDev {
     DomainDev d;
     float* buf[2][3];  // ping-pong h, hu, hv planes
     int64_t pitch;
     Control* ctl;
-    Partial* parts;
+    LedgerSlot* slots;  // ncta * warps per CTA
     int nstrips, rows_per_warp, ncta;
 };
+
+// One item of a batched step: warp `wib` of slot `slot` of member `md`.
+template <class M, int THREADS, bool MASKED>
+__device__ __forceinline__ void ensemble_item(const MemberDev& md, int slot, int par, WarpSmem& sm) {
+    constexpr int NW = THREADS / kWarp;
+    const int wib = threadIdx.x >> 5;
+    const int gw = slot * NW + wib;
+    __syncwarp();  // the previous item's slot copy has been read
+    ledger_prefetch(&md.slots[gw], sm.old);
+    cp_async_commit();
+    const PlanInputs pin = plan_fetch(md.ctl, par);
+    StepPlan pl;
+    auto plan_fn = [&]() -> MarchPlan {
+        pl = plan_step(md.d, pin);
+        if (slot == 0 && wib == 0) lead_advance(md.ctl, par, pin, pl);
+        return MarchPlan{pl.s, pl.snap, pl.dt, pl.go};
+    };
+    const int strip = gw % md.nstrips;
+    const int chunk = gw / md.nstrips;
+    const int r0 = chunk * md.rows_per_warp;
+    const int r1 = min(r0 + md.rows_per_warp, md.d.rows);
+    const StateView in{md.buf[par][0], md.buf[par][1], md.buf[par][2], md.pitch};
+    const StateOut out{md.buf[par ^ 1][0], md.buf[par ^ 1][1], md.buf[par ^ 1][2], md.pitch};
+    StepAccum acc;
+    acc.zero();
+    const bool went = r0 < md.d.rows ? march_pair<M, true, MASKED>(md.d, in, out, plan_fn, md.ctl, r0, r1,
+                                                                   strip * kWarp * 2, sm, acc)
+                                     : plan_fn().go != 0;
+    if (!went) {
+        cp_async_wait<0>();
+        return;
+    }
+    Accum a;
+    a.maxinv = acc.maxinv;
+    a.vol = acc.vol;
+    a.rain = acc.rain + (double)acc.rain_cells * (double)pl.s.dt_rain;
+    a.outflow = acc.outflow;
+    a.clip = acc.clip;
+    a.mask = acc.mask;
+    cp_async_wait<0>();
+    __syncwarp();
+    warp_end_step(md.ctl, &md.slots[gw], sm.old, par, pin.pos.steps, gw % kMaxStripes, a);
+}
 
 // The ensemble kernel keeps member fields in registers on top of the march.
 // At 4 CTAs/SM (128 registers) it spills a few words but, with marches of
@@ -490,35 +568,10 @@ ensemble_step_kernel(const MemberDev* __restrict__ members, const int2* __restri
     const int wib = threadIdx.x >> 5;
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const int2 item = items[it];
-        const Control* c = members[item.x].ctl;
-        if (*((volatile const int*)&c->done)) continue;  // uniform for the CTA
         __syncthreads();  // the previous item is done with s_md
         if (threadIdx.x == 0) s_md = members[item.x];
         __syncthreads();
-        const MemberDev& md = s_md;
-        const StepScalars s = c->s;
-        const int snap = c->snap;
-        const double dtd = c->dt;
-        const int gw = item.y * NW + wib;
-        const int strip = gw % md.nstrips;
-        const int chunk = gw / md.nstrips;
-        const int r0 = chunk * md.rows_per_warp;
-        const int r1 = min(r0 + md.rows_per_warp, md.d.rows);
-        const StateView in{md.buf[parity][0], md.buf[parity][1], md.buf[parity][2], md.pitch};
-        const StateOut out{md.buf[parity ^ 1][0], md.buf[parity ^ 1][1], md.buf[parity ^ 1][2], md.pitch};
-        StepAccum acc;
-        acc.zero();
-        if (r0 < md.d.rows)
-            march_pair<M, true, MASKED>(md.d, in, out, s, snap, dtd, md.ctl, r0, r1, strip * kWarp * 2,
-                                        s_warp[wib], acc);
-        Accum a;
-        a.maxinv = acc.maxinv;
-        a.vol = acc.vol;
-        a.rain = acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
-        a.outflow = acc.outflow;
-        a.clip = acc.clip;
-        a.mask = acc.mask;
-        finish_run_step<THREADS, 1>(md.d, md.ctl, md.parts, a, false, item.y, md.ncta);
+        ensemble_item<M, THREADS, MASKED>(s_md, item.y, parity, s_warp[wib]);
     }
 }
 
@@ -528,7 +581,7 @@ ensemble_step_kernel(const MemberDev* __restrict__ members, const int2* __restri
 // which the march reads as operands instead of holding them in registers.
 // Work items are numbered member after member; cta_begin[m] is member m's
 // first item, so a CTA finds its item's member by walking forward (its items
-// ascend).
+// ascend).  The warps of a CTA never wait for one another.
 constexpr int kEnsParamMembers = 96;
 struct EnsParams {
     MemberDev m[kEnsParamMembers];
@@ -546,35 +599,7 @@ ensemble_step_kernel_p(const __grid_constant__ EnsParams p) {
     int member = 0;
     for (int it = blockIdx.x; it < p.n_items; it += gridDim.x) {
         while (it >= p.cta_begin[member + 1]) ++member;
-        const MemberDev& md = p.m[member];
-        const int slot = it - p.cta_begin[member];
-        const Control* c = md.ctl;
-        if (*((volatile const int*)&c->done)) continue;  // uniform for the CTA
-        const StepScalars s = c->s;
-        const int snap = c->snap;
-        const double dtd = c->dt;
-        const int gw = slot * NW + wib;
-        const int strip = gw % md.nstrips;
-        const int chunk = gw / md.nstrips;
-        const int r0 = chunk * md.rows_per_warp;
-        const int r1 = min(r0 + md.rows_per_warp, md.d.rows);
-        const int par = p.parity;
-        const StateView in{md.buf[par][0], md.buf[par][1], md.buf[par][2], md.pitch};
-        const StateOut out{md.buf[par ^ 1][0], md.buf[par ^ 1][1], md.buf[par ^ 1][2], md.pitch};
-        StepAccum acc;
-        acc.zero();
-        if (r0 < md.d.rows)
-            march_pair<M, true, MASKED>(md.d, in, out, s, snap, dtd, md.ctl, r0, r1, strip * kWarp * 2,
-                                        s_warp[wib], acc);
-        Accum a;
-        a.maxinv = acc.maxinv;
-        a.vol = acc.vol;
-        a.rain = acc.rain + (double)acc.rain_cells * (double)s.dt_rain;
-        a.outflow = acc.outflow;
-        a.clip = acc.clip;
-        a.mask = acc.mask;
-        finish_run_step<THREADS, 1>(md.d, md.ctl, md.parts, a, false, slot, md.ncta);
-        __syncthreads();  // the fold's shared scratch is free before the next item
+        ensemble_item<M, THREADS, MASKED>(p.m[member], it - p.cta_begin[member], p.parity, s_warp[wib]);
     }
 }
 

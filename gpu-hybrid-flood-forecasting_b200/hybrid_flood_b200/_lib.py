@@ -38,6 +38,7 @@ EXPORTS = (
     "swe_last_launch_count",
     "swe_resident_load",
     "swe_resident_steps",
+    "swe_resident_prepare",
     "swe_resident_store",
     "swe_set_timing",
     "swe_last_step_time",
@@ -161,6 +162,7 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_last_launch_count": (ctypes.c_int64, [_vp]),
         "swe_resident_load": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, _f64, _vp]),
         "swe_resident_steps": (ctypes.c_int, [_vp, _i32, _vp]),
+        "swe_resident_prepare": (ctypes.c_int, [_vp, _i32]),
         "swe_resident_store": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i64, ctypes.POINTER(RunResult), _vp]),
         "swe_set_timing": (ctypes.c_int, [_vp, _i32]),
         "swe_last_step_time": (ctypes.c_int, [_vp, ctypes.POINTER(_f64), ctypes.POINTER(_i64)]),

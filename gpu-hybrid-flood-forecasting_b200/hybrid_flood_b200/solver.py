@@ -367,6 +367,12 @@ class B200ShallowWaterSolver:
             rc = self._lib.swe_resident_steps(self._handle, int(n_steps), _stream(self.device))
         _lib.check(rc, "resident_steps")
 
+    def resident_prepare(self, n_steps: int) -> None:
+        """Capture the step graphs the next ``n_steps`` resident steps use, without running them."""
+        with torch.cuda.device(self.device):
+            rc = self._lib.swe_resident_prepare(self._handle, int(n_steps))
+        _lib.check(rc, "resident_prepare")
+
     def resident_store(self, state: SWEState) -> tuple[float, int, dict]:
         """Copy the resident state into ``state`` (device tensors); ``(time, steps since load, ledger)``."""
         for t in state:

@@ -146,7 +146,11 @@ int swe_advance(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, i
  *   swe_resident_load   copies (h, hu, hv) in and starts the float64 clock at
  *                       start_s (the initial CFL reduction is enqueued);
  *   swe_resident_steps  enqueues n_steps CFL-limited steps and returns without
- *                       waiting (whole 32-step CUDA graphs where possible);
+ *                       waiting (as CUDA graphs of up to 32 steps, captured on
+ *                       first use);
+ *   swe_resident_prepare captures, without running anything, the graphs that
+ *                       the next n_steps steps will use, so that the later
+ *                       swe_resident_steps only launches;
  *   swe_resident_store  copies the current state out and reports the clock,
  *                       the steps taken since the load and the FP64 ledger
  *                       (it synchronises the stream).
@@ -155,6 +159,7 @@ int swe_advance(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, i
 int swe_resident_load(swe_domain_t d, const float *h, const float *hu, const float *hv, int64_t pitch,
                       double start_s, void *stream);
 int swe_resident_steps(swe_domain_t d, int32_t n_steps, void *stream);
+int swe_resident_prepare(swe_domain_t d, int32_t n_steps);
 int swe_resident_store(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch,
                        swe_run_result *result, void *stream);
 

@@ -22,19 +22,28 @@ def _net(seed=0):
     return net
 
 
-def test_fused_epilogue_matches_torch_ops_forward_and_backward(cuda_device):
+def test_fused_epilogue_matches_torch_ops_forward_and_backward(cuda_device, monkeypatch):
+    # Both networks run channels-last, so their convolutions are the same cuDNN
+    # calls and give the same pre-activations; only the epilogue differs (the
+    # reference's runs as torch ops).  With different convolution layouts an
+    # activation within rounding of zero can fall on either side of the ReLU,
+    # which moves a weight gradient by far more than rounding.
+    from hybrid_flood_b200 import unet
+
     torch.backends.cudnn.allow_tf32 = False
     torch.backends.cuda.matmul.allow_tf32 = False
-    ref = _net().to(cuda_device)  # NCHW: the epilogue runs as torch ops
+    ref = _net().to(cuda_device, memory_format=torch.channels_last)
     fused = _net().to(cuda_device, memory_format=torch.channels_last)
-    x = torch.randn(2, 5, 37, 45, device=cuda_device)
-    y_ref = ref(x)
-    y = fused(x.contiguous(memory_format=torch.channels_last))
-    torch.testing.assert_close(y, y_ref, rtol=1e-4, atol=1e-4)
+    x = torch.randn(2, 5, 37, 45, device=cuda_device).contiguous(memory_format=torch.channels_last)
+    with monkeypatch.context() as m:
+        m.setattr(unet, "_fusable", lambda y: False)
+        y_ref = ref(x)
+    y = fused(x)
+    torch.testing.assert_close(y, y_ref, rtol=1e-5, atol=1e-6)
     y_ref.square().mean().backward()
     y.square().mean().backward()
     for (n, a), (_, b) in zip(ref.named_parameters(), fused.named_parameters()):
-        torch.testing.assert_close(b.grad, a.grad, rtol=1e-3, atol=1e-5, msg=n)
+        torch.testing.assert_close(b.grad, a.grad, rtol=1e-4, atol=1e-6, msg=lambda m, n=n: f"{n}: {m}")
 
 
 def test_fused_epilogue_bf16_and_odd_channels(cuda_device):
