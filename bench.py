@@ -86,6 +86,8 @@ def _args():
     ap.add_argument("--no-training", action="store_true")
     ap.add_argument("--training-members", type=int, default=16)
     ap.add_argument("--training-size", type=int, default=1024)
+    ap.add_argument("--no-aux", action="store_true", help="skip the timing of the kernels around the step")
+    ap.add_argument("--aux-size", type=int, default=4096)
     ap.add_argument("--decompose", action="store_true",
                     help="also time the single domain split into row strips, one per GPU over NCCL (strong scaling)")
     return ap.parse_args()
@@ -482,6 +484,90 @@ def _adjoint(args, dev):
             "loss": float(loss.detach()), "grad_n_norm": float(n_t.grad.norm()), "grad_rain_scale": float(s_t.grad)}
 
 
+def _aux(args, dev):
+    """Device time and achieved bandwidth of the kernels around the step, each on an
+    aux_size x aux_size urban field (default 4096^2, inputs larger than the L2): the
+    run-start CFL/volume reduction, the allocation-free CFL reduction, the output
+    schema fields, the network features (5 channels, bf16), the volume-preserving
+    correction, the smoothed log-normal field and the urban DEM generator.  Each is
+    timed with CUDA events around `reps` back-to-back calls through the public API;
+    bytes are the kernels' algorithmic traffic per cell (reads + writes)."""
+    import ctypes
+
+    import torch
+
+    from hybrid_flood_b200 import _lib
+    from hybrid_flood_b200.generators import lognormal_field_device, member_fields, street_depth_device, urban_device
+    from hybrid_flood_b200.hybrid import HybridInputs, apply_residual_correction, network_features
+    from hybrid_flood_b200.output import output_fields
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver
+
+    n = args.aux_size
+    cells = n * n
+    peak, kind = _peaks()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+
+    def entry(name, ms, bytes_per_cell, note):
+        gbs = bytes_per_cell * cells / (ms / 1e3) / 1e9
+        out[name] = {"ms": ms, "bytes_per_cell": bytes_per_cell, "achieved_gbs": gbs, "frac": gbs / peak,
+                     "note": note}
+
+    member = urban_device(n, n, device=dev)
+    ms = timed(lambda: urban_device(n, n, device=dev), 3)
+    entry("urban_dem", ms, 9, "rectangle draws, first cover per cell, bed + Manning n + block mask written "
+                              "(9 B/cell); includes the hyetograph's copy to the host")
+    ms = timed(lambda: lognormal_field_device((n, n), median=0.03, sigma_log=0.4, seed=5, device=dev), 5)
+    entry("lognormal_field", ms, 44, "normal draws (8 B), two smoothing passes (2 x 16 B), moments and the "
+                                     "log-normal map (12 B), float64 intermediates")
+    solver = B200ShallowWaterSolver(**member_fields(member), arithmetic=args.arith, device=dev)
+    state = solver.initial_state(depth_m=street_depth_device(member))
+    solver.advance_(state, 20, 0.0)
+    ms = timed(lambda: solver.max_inverse_dt(state), 10)
+    entry("reduce_kernel", ms, 16, "run-start CFL maximum and volume: h, hu, hv and n^2 read; "
+                                   "the call returns the value to the host")
+    lib = _lib.load()
+    mask = torch.ones((n, n), dtype=torch.uint8, device=dev)
+    res = torch.empty(1, dtype=torch.float32, device=dev)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def noalloc():
+        _lib.check(lib.swe_max_inverse_dt_noalloc(ptr(state.h), ptr(state.hu), ptr(state.hv), n, ptr(mask), n, n,
+                                                   9.81, 1.0e-3, 1.0, 1.0, ptr(res), sp), "noalloc")
+
+    if cells <= 16_777_216:
+        entry("max_inverse_dt_noalloc_kernel", timed(noalloc, 10), 13, "h, hu, hv and the mask byte read")
+    fields = torch.empty((4, n, n), dtype=torch.float32, device=dev)
+    entry("schema_kernel", timed(lambda: output_fields(solver, state, fields), 10), 32,
+          "h, hu, hv and n^2 (mask) read (16 B), depth, u, v, speed written (16 B)")
+    hi = HybridInputs(None, None, np.zeros(5, np.float32), np.ones(5, np.float32), 1.0, np.ones(3, np.float32))
+    feats = torch.empty((1, n, n, 5), dtype=torch.bfloat16, device=dev)
+    entry("features_kernel", timed(lambda: network_features(solver, state, hi, 600.0, layout="state5",
+                                                            dtype=torch.bfloat16, out=feats), 10), 30,
+          "h, hu, hv, n^2 (mask) and bed read (20 B), 5 bf16 channels written (10 B)")
+    resid = torch.zeros((n, n, 3), dtype=torch.bfloat16, device=dev)
+    corr = type(state)(*(torch.empty_like(t) for t in state))
+    entry("correction", timed(lambda: apply_residual_correction(solver, state, resid, correction_relaxation=0.5,
+                                                                out=corr), 10), 56,
+          "sums pass: n^2, h and the bf16 residual's sectors read, provisional depth written (18 B); "
+          "apply pass: n^2, h, hu, hv, provisional depth and the residual read, new state written (38 B)")
+    return {"size": [n, n], "peak_gbs": peak, "peak_kind": kind, "kernels": out,
+            "timing": "CUDA events around back-to-back calls of the public API (host work between calls included)"}
+
+
 def _hybrid(args, dev):
     """Coupled physics + corrector rollout: 16 urban 1024x1024 members, the
     4-level (32/64/128/256) bfloat16 channels_last corrector on (h, hu, hv, z,
@@ -791,6 +877,9 @@ def run_b200(args, rank: int, world: int):
     par = None
     if not args.no_parity and rank == 0:
         par = _parity(args, w, depth, dev)
+    aux = None
+    if not args.no_aux and rank == 0:
+        aux = _aux(args, dev)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -831,6 +920,8 @@ def run_b200(args, rank: int, world: int):
         line["decomposed"] = dec
     if trn:
         line["training"] = trn
+    if aux:
+        line["aux_kernels"] = aux
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = _cpu_legs(w, depth)
     print(json.dumps(line), flush=True)

@@ -38,6 +38,22 @@ __device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ float2 vmax(float2 a, float2 b) { return {fmaxf(a.x, b.x), fmaxf(a.y, b.y)}; }
 __device__ __forceinline__ float vmin(float a, float b) { return fminf(a, b); }
 __device__ __forceinline__ float2 vmin(float2 a, float2 b) { return {fminf(a.x, b.x), fminf(a.y, b.y)}; }
+// Three-input minimum / maximum (one sm_100 instruction each; NaN inputs are
+// ignored as by fminf / fmaxf).
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float vmin3(float a, float b, float c) { return min3f(a, b, c); }
+__device__ __forceinline__ float2 vmin3(float2 a, float2 b, float2 c) { return {min3f(a.x, b.x, c.x), min3f(a.y, b.y, c.y)}; }
+__device__ __forceinline__ float vmax3(float a, float b, float c) { return max3f(a, b, c); }
+__device__ __forceinline__ float2 vmax3(float2 a, float2 b, float2 c) { return {max3f(a.x, b.x, c.x), max3f(a.y, b.y, c.y)}; }
 __device__ __forceinline__ float vabs(float a) { return fabsf(a); }
 __device__ __forceinline__ float2 vabs(float2 a) { return {fabsf(a.x), fabsf(a.y)}; }
 __device__ __forceinline__ float neg(float a) { return -a; }
@@ -210,8 +226,6 @@ __device__ __forceinline__ FaceT<T> face_t(const CellT<T>& lo, const CellT<T>& h
     }
     const T cL = A::sqrt(A::mul(kp.g, HL));
     const T cR = A::sqrt(A::mul(kp.g, HR));
-    const T sL = vmin(A::sub(unL, cL), A::sub(unR, cR));
-    const T sR = vmax(A::add(unL, cL), A::add(unR, cR));
     const T pL = A::mul(kp.half_g, A::mul(HL, HL));
     const T pR = A::mul(kp.half_g, A::mul(HR, HR));
     T fL0, fL1, fL2, fR0, fR1, fR2;
@@ -242,6 +256,8 @@ __device__ __forceinline__ FaceT<T> face_t(const CellT<T>& lo, const CellT<T>& h
     }
     FaceT<T> f;
     if constexpr (A::kExact) {
+        const T sL = vmin(A::sub(unL, cL), A::sub(unR, cR));
+        const T sR = vmax(A::add(unL, cL), A::add(unR, cR));
         const T spread = A::sub(sR, sL);
         const T den = sel(gt(spread, kp.eps), spread, kp.one);
         const T s01 = A::mul(sL, sR);
@@ -255,9 +271,14 @@ __device__ __forceinline__ FaceT<T> face_t(const CellT<T>& lo, const CellT<T>& h
         f.corr_lo = sel(relevant, A::mul(kp.half_g, A::sub(A::mul(hL, hL), A::mul(HL, HL))), kp.zero);
         f.corr_hi = sel(relevant, A::mul(kp.half_g, A::sub(A::mul(hR, hR), A::mul(HR, HR))), kp.zero);
     } else {
-        // Clamped speeds: sL >= 0 gives fL, sR <= 0 gives fR, otherwise the HLL middle state.
-        const T sm = vmin(sL, kp.zero), sp = vmax(sR, kp.zero);
-        const T rden = A::rcp(vmax(A::sub(sp, sm), kp.tiny));
+        // Clamped speeds: sL >= 0 gives fL, sR <= 0 gives fR, otherwise the HLL
+        // middle state.  s- = min(sL, 0) and s+ = max(sR, 0) are each one
+        // three-input instruction; s+ - s- >= 0, and the tiny term keeps the
+        // reciprocal finite where both speeds are zero (a still, dry face, whose
+        // flux terms are then all zero).
+        const T sm = vmin3(A::sub(unL, cL), A::sub(unR, cR), kp.zero);
+        const T sp = vmax3(A::add(unL, cL), A::add(unR, cR), kp.zero);
+        const T rden = A::rcp(A::add(A::sub(sp, sm), kp.tiny));
         const T smp = A::mul(sm, sp);
         const T nsm = neg(sm);
         T m0 = A::fma(smp, A::sub(HR, HL), A::fma(nsm, fR0, A::mul(sp, fL0)));

@@ -39,7 +39,7 @@ constexpr int kRing = 4;  // rows in flight per warp (a power of two)
 // batch and the cp.async row ring.
 struct WarpSmem {
     float left[3][kWarp];      // hi side of the strip's left x-face, per batch row
-    float right[7][kWarp];     // the cell right of the strip, per batch row
+    float right[5][kWarp];     // the cell right of the strip, per batch row: h, z, n^2, u, v
     float2 ring[kRing][5][kWarp];  // [slot][field][lane]
     double led[5][kWarp];      // float64 ledger sums per lane (vol, rain, clip, mask, outflow)
     alignas(16) double old[4]; // the warp's ledger slot as the step found it (run mode)
@@ -196,21 +196,21 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
         float2 e0;          // mass flux through each cell's right face (east outflow)
     };
     auto xfaces = [&](const CellT<float2>& cur, int j) -> XF {
+        // The face reads depth, bed and velocities of its two cells (and n^2 for
+        // the mask): the neighbour's momenta are not moved.
         float rh = __shfl_down_sync(0xffffffffu, cur.h.x, 1);
-        float rhu = __shfl_down_sync(0xffffffffu, cur.hu.x, 1);
-        float rhv = __shfl_down_sync(0xffffffffu, cur.hv.x, 1);
         float rz = __shfl_down_sync(0xffffffffu, cur.z.x, 1);
-        float rnm = __shfl_down_sync(0xffffffffu, cur.nm.x, 1);
+        float rnm = MASKED ? __shfl_down_sync(0xffffffffu, cur.nm.x, 1) : 0.f;
         float ru = __shfl_down_sync(0xffffffffu, cur.u.x, 1);
         float rv = __shfl_down_sync(0xffffffffu, cur.v.x, 1);
         if (lane == 31) {
-            rh = sm.right[0][j]; rhu = sm.right[1][j]; rhv = sm.right[2][j]; rz = sm.right[3][j];
-            rnm = sm.right[4][j]; ru = sm.right[5][j]; rv = sm.right[6][j];
+            rh = sm.right[0][j]; rz = sm.right[1][j]; ru = sm.right[3][j]; rv = sm.right[4][j];
+            if (MASKED) rnm = sm.right[2][j];
         }
         CellT<float2> xhi;
         xhi.h = f2(cur.h.y, rh);
-        xhi.hu = f2(cur.hu.y, rhu);
-        xhi.hv = f2(cur.hv.y, rhv);
+        xhi.hu = kp.zero;
+        xhi.hv = kp.zero;
         xhi.z = f2(cur.z.y, rz);
         xhi.nm = f2(cur.nm.y, rnm);
         xhi.u = f2(cur.u.y, ru);
@@ -358,12 +358,10 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
         sm.left[2][lane] = f.f2;
         if (RUN && x0w == 0 && rb + lane < r1) lg.out_x.x -= f.f0;
         sm.right[0][lane] = q.h;
-        sm.right[1][lane] = q.hu;
-        sm.right[2][lane] = q.hv;
-        sm.right[3][lane] = q.z;
-        sm.right[4][lane] = q.nm;
-        sm.right[5][lane] = q.u;
-        sm.right[6][lane] = q.v;
+        sm.right[1][lane] = q.z;
+        sm.right[2][lane] = q.nm;
+        sm.right[3][lane] = q.u;
+        sm.right[4][lane] = q.v;
         __syncwarp();
     };
 

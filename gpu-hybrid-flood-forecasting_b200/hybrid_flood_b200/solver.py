@@ -246,11 +246,15 @@ class B200ShallowWaterSolver:
 
     # -- reference surface --------------------------------------------------
     def initial_state(self, *, depth_m=0.0, x_velocity_m_s=0.0, y_velocity_m_s=0.0) -> SWEState:
-        """Masked conserved fields from depth and velocity inputs."""
+        """Masked conserved fields from depth and velocity inputs (scalars, arrays or tensors)."""
         f32 = dict(dtype=torch.float32, device=self.device)
-        depth = torch.as_tensor(np.asarray(depth_m, dtype=np.float32), **f32).broadcast_to(self.shape)
-        u = torch.as_tensor(np.asarray(x_velocity_m_s, dtype=np.float32), **f32).broadcast_to(self.shape)
-        v = torch.as_tensor(np.asarray(y_velocity_m_s, dtype=np.float32), **f32).broadcast_to(self.shape)
+
+        def field(x):
+            if isinstance(x, torch.Tensor):
+                return x.to(**f32).broadcast_to(self.shape)
+            return torch.as_tensor(np.asarray(x, dtype=np.float32), **f32).broadcast_to(self.shape)
+
+        depth, u, v = field(depth_m), field(x_velocity_m_s), field(y_velocity_m_s)
         depth = torch.where(self.domain_mask, torch.clamp_min(depth, 0.0), torch.zeros((), **f32))
         return SWEState(depth.contiguous(), (depth * u).contiguous(), (depth * v).contiguous())
 

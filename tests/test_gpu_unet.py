@@ -27,11 +27,14 @@ def test_fused_epilogue_matches_torch_ops_forward_and_backward(cuda_device, monk
     # calls and give the same pre-activations; only the epilogue differs (the
     # reference's runs as torch ops).  With different convolution layouts an
     # activation within rounding of zero can fall on either side of the ReLU,
-    # which moves a weight gradient by far more than rounding.
+    # which moves a weight gradient by far more than rounding.  Deterministic
+    # cuDNN algorithms keep the weight gradients' summation order the same in
+    # both (the default ones may add split partial sums in any order).
     from hybrid_flood_b200 import unet
 
     torch.backends.cudnn.allow_tf32 = False
     torch.backends.cuda.matmul.allow_tf32 = False
+    monkeypatch.setattr(torch.backends.cudnn, "deterministic", True)
     ref = _net().to(cuda_device, memory_format=torch.channels_last)
     fused = _net().to(cuda_device, memory_format=torch.channels_last)
     x = torch.randn(2, 5, 37, 45, device=cuda_device).contiguous(memory_format=torch.channels_last)
@@ -43,7 +46,10 @@ def test_fused_epilogue_matches_torch_ops_forward_and_backward(cuda_device, monk
     y_ref.square().mean().backward()
     y.square().mean().backward()
     for (n, a), (_, b) in zip(ref.named_parameters(), fused.named_parameters()):
-        torch.testing.assert_close(b.grad, a.grad, rtol=1e-4, atol=1e-6, msg=lambda m, n=n: f"{n}: {m}")
+        # Rounding of a sum of ~3000 products, well below the effect of a wrong
+        # mask element or bias term (relative 1e-2 and more).
+        atol = 1e-5 * float(a.grad.abs().max())
+        torch.testing.assert_close(b.grad, a.grad, rtol=1e-3, atol=atol, msg=lambda m, n=n: f"{n}: {m}")
 
 
 def test_fused_epilogue_bf16_and_odd_channels(cuda_device):
