@@ -258,18 +258,32 @@ void launch_step(const swe_domain* d, const Plan& pl, const StepLaunch& sl, bool
     dispatch(pl.V, d->arith, run, d->masked, [&](auto k) { decltype(k)::launch(pl.blocks, sl, st); });
 }
 
+// 2-D grid of a per-cell kernel over rows x cols (for_cells): x over the
+// columns, y over the rows, about 8 CTAs per SM (and about `per_thread` cells
+// per thread on small planes).
+dim3 cell_grid(int rows, int cols, int threads, int sms, int per_thread = 1) {
+    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((cols + threads - 1) / threads, (int64_t)sms * 8));
+    const int64_t want = std::max<int64_t>(1, ((int64_t)rows * cols + (int64_t)threads * per_thread - 1) /
+                                                  ((int64_t)threads * per_thread) / gx);
+    const int64_t gy = std::max<int64_t>(1, std::min<int64_t>({(int64_t)rows, want, ((int64_t)sms * 8 + gx - 1) / gx}));
+    return dim3((unsigned)gx, (unsigned)gy);
+}
+
+dim3 reduce_grid(const swe_domain* d) {
+    return cell_grid(d->dd.upd_hi - d->dd.upd_lo, d->dd.cols, kThreads, d->sms, 8);
+}
+
 int reduce_blocks(const swe_domain* d) {
-    const int64_t n = (int64_t)d->dd.rows * d->dd.cols;
-    const int64_t want = (n + kThreads * 8 - 1) / (kThreads * 8);
-    return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)d->sms * 8));
+    const dim3 g = reduce_grid(d);
+    return (int)(g.x * g.y);
 }
 
 void launch_reduce(const swe_domain* d, const StateView& s, Control* ctl, cudaStream_t st) {
-    const int blocks = reduce_blocks(d);
+    const dim3 grid = reduce_grid(d);
     if (d->arith == SWE_ARITH_FAST)
-        reduce_kernel<FastMath, kThreads><<<blocks, kThreads, 0, st>>>(d->dd, s, ctl, d->rparts);
+        reduce_kernel<FastMath, kThreads><<<grid, kThreads, 0, st>>>(d->dd, s, ctl, d->rparts);
     else
-        reduce_kernel<ExactMath, kThreads><<<blocks, kThreads, 0, st>>>(d->dd, s, ctl, d->rparts);
+        reduce_kernel<ExactMath, kThreads><<<grid, kThreads, 0, st>>>(d->dd, s, ctl, d->rparts);
 }
 
 int choose_vec(const void* const* ptrs, int n, int64_t pitch_a, int64_t pitch_b) {
@@ -1605,9 +1619,7 @@ int swe_network_features(swe_domain_t d, const float* h, const float* hu, const 
     a.channels = layout == kFeatRef6 ? 6 : 5;
     a.out = out;
     a.out_bf16 = out_bf16 ? 1 : 0;
-    const int64_t n = (int64_t)a.rows * a.cols;
-    features_kernel<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)d->sms * 8), 256, 0,
-                      static_cast<cudaStream_t>(stream)>>>(a);
+    features_kernel<<<cell_grid(a.rows, a.cols, 256, d->sms), 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
     SWE_CK(cudaGetLastError());
     return SWE_OK;
 }
@@ -1631,9 +1643,7 @@ int swe_output_fields(swe_domain_t d, const float* h, const float* hu, const flo
     a.v = y_velocity;
     a.speed = speed;
     a.out_pitch = out_pitch;
-    const int64_t n = (int64_t)a.rows * a.cols;
-    schema_kernel<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)d->sms * 8), 256, 0,
-                    static_cast<cudaStream_t>(stream)>>>(a);
+    schema_kernel<<<cell_grid(a.rows, a.cols, 256, d->sms), 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
     SWE_CK(cudaGetLastError());
     return SWE_OK;
 }
@@ -1702,10 +1712,9 @@ int swe_apply_correction(swe_domain_t d, const float* h, const float* hu, const 
     a.dry = d->dd.k.dry;
     a.eps = 1.1920929e-07f;  // float32 machine epsilon (jnp.finfo(float32).eps)
     a.sums = d->corr_sums;
-    const int64_t n = (int64_t)a.rows * a.cols;
-    const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)d->sms * 8);
-    correction_sums_kernel<<<blocks, 256, 0, st>>>(a);
-    correction_apply_kernel<<<blocks, 256, 0, st>>>(a);
+    const dim3 grid = cell_grid(a.rows, a.cols, 256, d->sms);
+    correction_sums_kernel<<<grid, 256, 0, st>>>(a);
+    correction_apply_kernel<<<grid, 256, 0, st>>>(a);
     SWE_CK(cudaGetLastError());
     return SWE_OK;
 }
@@ -2083,11 +2092,45 @@ int swe_last_step_time(swe_domain_t d, double* ms, int64_t* step_launches) {
 namespace {
 
 // Device scratch that frees itself (the generators are set-up calls).
+// Scratch of the generators: a stream-ordered memory pool of the library's own
+// per device, which keeps freed blocks for the next call (a plain cudaFree
+// synchronises the whole device and returns the pages, which cost more than
+// the generator's kernels).  Blocks are freed in stream order when the buffer
+// goes out of scope, so a call returns without waiting for its kernels.
+cudaMemPool_t scratch_pool(int dev) {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)pools.size() <= dev) pools.resize((size_t)dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = p;
+    }
+    return pools[dev];
+}
+
 template <class T>
 struct DevBuf {
     T* p = nullptr;
-    ~DevBuf() { cudaFree(p); }
-    cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * std::max<size_t>(n, 1)); }
+    cudaStream_t st = nullptr;
+    ~DevBuf() {
+        if (p) cudaFreeAsync(p, st);
+    }
+    cudaError_t alloc(size_t n, cudaStream_t s) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaMemPool_t pool = scratch_pool(dev);
+        if (!pool) return cudaErrorMemoryAllocation;
+        st = s;
+        return cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), sizeof(T) * std::max<size_t>(n, 1), pool, s);
+    }
 };
 
 int gen_blocks(int64_t work, int sms) {
@@ -2119,7 +2162,7 @@ int swe_generate_urban(const swe_urban_desc* q, float* bed, float* manning_n, ui
     const int64_t cells = (int64_t)rows * cols;
     const double target = q->coverage * (double)cells;
     DevBuf<int> first;
-    SWE_CK(first.alloc((size_t)cells));
+    SWE_CK(first.alloc((size_t)cells, st));
     int n_blocks = 0;
     // Drawn rectangles: a first batch about twice the expected need, doubled until it reaches the target.
     const double side = 0.5 * (q->min_side + q->max_side);
@@ -2129,8 +2172,8 @@ int swe_generate_urban(const swe_urban_desc* q, float* bed, float* manning_n, ui
     for (;;) {
         DevBuf<Rect> rects;
         DevBuf<int> counts;
-        SWE_CK(rects.alloc((size_t)n));
-        SWE_CK(counts.alloc((size_t)n));
+        SWE_CK(rects.alloc((size_t)n, st));
+        SWE_CK(counts.alloc((size_t)n, st));
         if (q->n_rects > 0) {
             std::vector<Rect> hr((size_t)n);
             for (int i = 0; i < n; ++i) {
@@ -2164,7 +2207,6 @@ int swe_generate_urban(const swe_urban_desc* q, float* bed, float* manning_n, ui
                                                               q->block_raise_m, q->street_offset_m, q->n_block,
                                                               q->n_street, q->n_scale, bed, manning_n, block_mask);
     SWE_CK(cudaGetLastError());
-    SWE_CK(cudaStreamSynchronize(st));  // the scratch is freed on return
     if (blocks_used) *blocks_used = n_blocks;
     return SWE_OK;
 }
@@ -2199,19 +2241,21 @@ int swe_generate_lognormal_field(int32_t rows, int32_t cols, double median, doub
     }
     for (auto& v : taps) v /= tsum;
     DevBuf<double> a, b, dtaps, partials, sums;
-    SWE_CK(a.alloc((size_t)cells));
-    SWE_CK(b.alloc((size_t)cells));
-    SWE_CK(dtaps.alloc(taps.size()));
-    SWE_CK(partials.alloc(kGenSumBlocks));
-    SWE_CK(sums.alloc(2));
+    SWE_CK(a.alloc((size_t)cells, st));
+    SWE_CK(b.alloc((size_t)cells, st));
+    SWE_CK(dtaps.alloc(taps.size(), st));
+    SWE_CK(partials.alloc(kGenSumBlocks, st));
+    SWE_CK(sums.alloc(2, st));
     SWE_CK(cudaMemcpyAsync(dtaps.p, taps.data(), sizeof(double) * taps.size(), cudaMemcpyHostToDevice, st));
     const double* src = noise;
     if (!src) {
         normal_field_kernel<<<gen_blocks(cells, sms), 256, 0, st>>>(seed, cells, a.p);
         src = a.p;
     }
-    smooth_pass_kernel<1><<<gen_blocks(cells, sms), 256, 0, st>>>(src, b.p, rows, cols, dtaps.p, radius);
-    smooth_pass_kernel<0><<<gen_blocks(cells, sms), 256, 0, st>>>(b.p, a.p, rows, cols, dtaps.p, radius);
+    const unsigned gx = (unsigned)std::min<int64_t>((cols + 255) / 256, (int64_t)sms * 8);
+    const dim3 sgrid(gx, (unsigned)std::max<int64_t>(1, std::min<int64_t>(rows, (int64_t)sms * 8 / gx)));
+    smooth_pass_kernel<1><<<sgrid, 256, 0, st>>>(src, b.p, rows, cols, dtaps.p, radius);
+    smooth_pass_kernel<0><<<sgrid, 256, 0, st>>>(b.p, a.p, rows, cols, dtaps.p, radius);
     // Two-pass moments: the mean, then the squared deviations from it.
     block_sums_kernel<256><<<kGenSumBlocks, 256, 0, st>>>(a.p, cells, nullptr, partials.p);
     fold_sums_kernel<<<1, 32, 0, st>>>(partials.p, kGenSumBlocks, sums.p);
@@ -2219,7 +2263,6 @@ int swe_generate_lognormal_field(int32_t rows, int32_t cols, double median, doub
     fold_sums_kernel<<<1, 32, 0, st>>>(partials.p, kGenSumBlocks, sums.p + 1);
     lognormal_finish_kernel<<<gen_blocks(cells, sms), 256, 0, st>>>(a.p, cells, sums.p, median, sigma_log, out);
     SWE_CK(cudaGetLastError());
-    SWE_CK(cudaStreamSynchronize(st));  // the scratch is freed on return
     return SWE_OK;
 }
 

@@ -215,19 +215,33 @@ __device__ __forceinline__ int reflect_index(int i, int n) {
 
 // One pass of the separable Gaussian (taps[0 .. 2*radius]) along rows (axis 1)
 // or columns (axis 0), reflect-padded, in float64 with the taps applied in
-// order from the lowest index.
+// order from the lowest index.  A 2-D grid (x: columns, y: rows, both
+// grid-strided) gives every thread its row and column without a division, and
+// only cells within `radius` of an edge take the reflected indices.
 template <int AXIS>
 __global__ void smooth_pass_kernel(const double* in, double* out, int rows, int cols, const double* taps, int radius) {
-    const int64_t total = (int64_t)rows * cols;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(i / cols), c = (int)(i % cols);
-        double acc = 0.0;
-        for (int t = -radius; t <= radius; ++t) {
-            const double v = AXIS == 1 ? in[(int64_t)r * cols + reflect_index(c + t, cols)]
-                                       : in[(int64_t)reflect_index(r + t, rows) * cols + c];
-            acc = __fma_rn(v, taps[t + radius], acc);
+    for (int r = blockIdx.y; r < rows; r += gridDim.y) {
+        const double* row = in + (int64_t)r * cols;
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
+            double acc = 0.0;
+            if (AXIS == 1) {
+                if (c >= radius && c + radius < cols) {
+                    for (int t = -radius; t <= radius; ++t) acc = __fma_rn(row[c + t], taps[t + radius], acc);
+                } else {
+                    for (int t = -radius; t <= radius; ++t)
+                        acc = __fma_rn(row[reflect_index(c + t, cols)], taps[t + radius], acc);
+                }
+            } else {
+                if (r >= radius && r + radius < rows) {
+                    const double* p = in + (int64_t)(r - radius) * cols + c;
+                    for (int t = 0; t <= 2 * radius; ++t) acc = __fma_rn(p[(int64_t)t * cols], taps[t], acc);
+                } else {
+                    for (int t = -radius; t <= radius; ++t)
+                        acc = __fma_rn(in[(int64_t)reflect_index(r + t, rows) * cols + c], taps[t + radius], acc);
+                }
+            }
+            out[(int64_t)r * cols + c] = acc;
         }
-        out[i] = acc;
     }
 }
 

@@ -36,9 +36,8 @@ struct FeatureArgs {
 };
 
 __global__ void features_kernel(const FeatureArgs a) {
-    const int64_t n = (int64_t)a.rows * a.cols;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(i / a.cols), c = (int)(i - (int64_t)r * a.cols);
+    for_cells(0, a.rows, a.cols, [&](int r, int c) {
+        const int64_t i = (int64_t)r * a.cols + c;
         const int64_t so = (int64_t)r * a.s.pitch + c, zo = (int64_t)r * a.spitch + c;
         const float h = a.s.h[so], hu = a.s.hu[so], hv = a.s.hv[so];
         const bool act = active(a.nm[zo]);
@@ -64,7 +63,7 @@ __global__ void features_kernel(const FeatureArgs a) {
             float* o = static_cast<float*>(a.out) + i * a.channels;
             for (int q = 0; q < a.channels; ++q) o[q] = f[q];
         }
-    }
+    });
 }
 
 struct CorrectionArgs {
@@ -96,10 +95,8 @@ __device__ __forceinline__ float residual_at(const CorrectionArgs& a, int r, int
 // Pass 1: provisional depth max(h + r*res_h, 0) on active cells (into the
 // scratch plane) and the two volume sums in float64 (coupled_forecast.py:98-104).
 __global__ void correction_sums_kernel(const CorrectionArgs a) {
-    const int64_t n = (int64_t)a.rows * a.cols;
     double t = 0.0, p = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(i / a.cols), c = (int)(i - (int64_t)r * a.cols);
+    for_cells(0, a.rows, a.cols, [&](int r, int c) {
         const int64_t so = (int64_t)r * a.s.pitch + c;
         const bool act = active(a.nm[(int64_t)r * a.spitch + c]);
         const float h = a.s.h[so];
@@ -108,7 +105,7 @@ __global__ void correction_sums_kernel(const CorrectionArgs a) {
         a.prov[(int64_t)r * a.prov_pitch + c] = prov;  // provisional depth, scaled in pass 2
         if (act) t += (double)h;
         p += (double)prov;
-    }
+    });
     t = warp_sum(t);
     p = warp_sum(p);
     __shared__ double s_t[32], s_p[32];
@@ -132,12 +129,10 @@ __global__ void correction_sums_kernel(const CorrectionArgs a) {
 // Pass 2: project onto the physics volume and rebuild the momenta
 // (coupled_forecast.py:105-120).  Reads the predicted momenta before writing.
 __global__ void correction_apply_kernel(const CorrectionArgs a) {
-    const int64_t n = (int64_t)a.rows * a.cols;
     const double target = a.sums[0], provisional = a.sums[1];
     const float scale = provisional > (double)a.eps ? (float)(target / provisional) : 1.f;
     const bool keep = !(target > (double)a.eps);
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(i / a.cols), c = (int)(i - (int64_t)r * a.cols);
+    for_cells(0, a.rows, a.cols, [&](int r, int c) {
         const int64_t so = (int64_t)r * a.s.pitch + c, oo = (int64_t)r * a.out.pitch + c;
         const bool act = active(a.nm[(int64_t)r * a.spitch + c]);
         const float h = a.s.h[so], hu = a.s.hu[so], hv = a.s.hv[so];
@@ -154,7 +149,7 @@ __global__ void correction_apply_kernel(const CorrectionArgs a) {
         a.out.h[oo] = ch;
         a.out.hu[oo] = wet ? __fmul_rn(ch, u) : 0.f;
         a.out.hv[oo] = wet ? __fmul_rn(ch, v) : 0.f;
-    }
+    });
 }
 
 // Output schema of a state (conserved_to_xarray, structured_io.py:160-209):
@@ -172,10 +167,8 @@ struct SchemaArgs {
 };
 
 __global__ void schema_kernel(const SchemaArgs a) {
-    const int64_t n = (int64_t)a.rows * a.cols;
     const float nan = __int_as_float(0x7fc00000);
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(i / a.cols), c = (int)(i - (int64_t)r * a.cols);
+    for_cells(0, a.rows, a.cols, [&](int r, int c) {
         const int64_t so = (int64_t)r * a.s.pitch + c, oo = (int64_t)r * a.out_pitch + c;
         const bool act = active(a.nm[(int64_t)r * a.spitch + c]);
         const float h = a.s.h[so];
@@ -186,7 +179,7 @@ __global__ void schema_kernel(const SchemaArgs a) {
         a.u[oo] = act ? u : nan;
         a.v[oo] = act ? v : nan;
         a.speed[oo] = act ? ExactMath::hypot(u, v) : nan;
-    }
+    });
 }
 
 }  // namespace swe

@@ -561,11 +561,11 @@ __device__ __forceinline__ Partial cta_reduce(Accum acc) {
 // PER: partials a thread of the last CTA loads before folding them.
 template <int THREADS, int PER = 8>
 __device__ void finish_start(const DomainDev& d, Control* ctl, Partial* parts, Accum acc) {
-    const int nparts = gridDim.x;
+    const int nparts = (int)(gridDim.x * gridDim.y);
     __shared__ bool s_last;
     const Partial p = cta_reduce<THREADS>(acc);
     if (threadIdx.x == 0) {
-        parts[blockIdx.x] = p;
+        parts[blockIdx.y * gridDim.x + blockIdx.x] = p;
         __threadfence();
         const unsigned ticket = atomicAdd(&ctl->counter, 1u);
         s_last = (ticket == (unsigned)nparts - 1);
@@ -1061,18 +1061,26 @@ __global__ void __launch_bounds__(THREADS, MinBlocks<V>::value) step_kernel(cons
     }
 }
 
+// Cells [r0, r1) x [0, cols) of a plane under a 2-D grid-stride launch (grid.x
+// over columns, grid.y over rows, see cell_grid on the host): body(r, c) for
+// each, with no division per cell.
+template <class F>
+__device__ __forceinline__ void for_cells(int r0, int r1, int cols, F&& body) {
+    for (int r = r0 + (int)blockIdx.y; r < r1; r += (int)gridDim.y)
+        for (int c = (int)(blockIdx.x * blockDim.x + threadIdx.x); c < cols; c += (int)(gridDim.x * blockDim.x))
+            body(r, c);
+}
+
 // Max inverse CFL dt and stored volume of a state (the reduction of
 // compute_cfl_dt, shallow_water_2d.py:269-273); initialises the run control.
+// A 2-D launch: each CTA's partial is slot blockIdx.y * gridDim.x + blockIdx.x.
 template <class M, int THREADS>
 __global__ void __launch_bounds__(THREADS) reduce_kernel(const DomainDev d, const StateView s,
                                                          Control* ctl, Partial* parts) {
     const Consts& k = d.k;
     Accum acc;
     acc.zero();
-    const int64_t n = (int64_t)(d.upd_hi - d.upd_lo) * d.cols;
-    for (int64_t i = (int64_t)blockIdx.x * THREADS + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * THREADS) {
-        const int r = d.upd_lo + (int)(i / d.cols), c = (int)(i - (int64_t)(r - d.upd_lo) * d.cols);
+    for_cells(d.upd_lo, d.upd_hi, d.cols, [&](int r, int c) {
         const float h = s.h[(int64_t)r * s.pitch + c];
         const float hu = s.hu[(int64_t)r * s.pitch + c];
         const float hv = s.hv[(int64_t)r * s.pitch + c];
@@ -1083,7 +1091,7 @@ __global__ void __launch_bounds__(THREADS) reduce_kernel(const DomainDev d, cons
         const float inv = M::add(M::div(M::add(fabsf(u), w), k.dx), M::div(M::add(fabsf(v), w), k.dy));
         acc.maxinv = nan_max(acc.maxinv, act ? inv : 0.0f);
         if (act) acc.vol += (double)h;
-    }
+    });
     finish_start<THREADS>(d, ctl, parts, acc);
 }
 
