@@ -38,7 +38,7 @@ constexpr int kRing = 4;  // rows in flight per warp (a power of two)
 // Warp-private shared memory of the march: strip edges of the current 32-row
 // batch and the cp.async row ring.
 struct WarpSmem {
-    float4 left[kWarp];        // hi side of the strip's left x-face per batch row: f0, f1, f2, -
+    float left[3][kWarp];      // hi side of the strip's left x-face, per batch row
     float right[5][kWarp];     // the cell right of the strip per batch row: h, z, n^2, u, v
     float2 ring[kRing][5][kWarp];  // [slot][field][lane]
     double led[5][kWarp];      // float64 ledger sums per lane (vol, rain, clip, mask, outflow)
@@ -221,8 +221,7 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
         float up1 = __shfl_up_sync(0xffffffffu, xh1.y, 1);
         float up2 = __shfl_up_sync(0xffffffffu, fx.f2.y, 1);
         if (lane == 0) {
-            const float4 e = sm.left[j];
-            up0 = e.x; up1 = e.y; up2 = e.z;
+            up0 = sm.left[0][j]; up1 = sm.left[1][j]; up2 = sm.left[2][j];
         }
         XF x;
         x.r0 = fx.f0;
@@ -354,7 +353,9 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
         set_vel_t<M>(e, ks);
         set_vel_t<M>(q, ks);
         const FaceT<float> f = face_t<1, M, MASKED>(l, e, ks);
-        sm.left[lane] = make_float4(f.f0, A::add(f.f1, f.corr_hi), f.f2, 0.f);
+        sm.left[0][lane] = f.f0;
+        sm.left[1][lane] = A::add(f.f1, f.corr_hi);
+        sm.left[2][lane] = f.f2;
         if (RUN && x0w == 0 && rb + lane < r1) lg.out_x.x -= f.f0;
         sm.right[0][lane] = q.h;
         sm.right[1][lane] = q.z;
