@@ -146,14 +146,16 @@ struct swe_domain {
 
 namespace {
 
-// Step kernels are launched with programmatic stream serialisation, so that a
-// step's launch overlaps the end of the previous step (the kernels wait for
-// their predecessor with griddepcontrol.wait before touching memory).
-// SWE_PDL=0 turns it off.
+// SWE_PDL=1 launches the step kernels with programmatic stream serialisation,
+// so that a step's CTAs are placed while the previous step ends (the kernels
+// wait for their predecessor with griddepcontrol.wait before touching memory;
+// without the attribute that instruction does nothing).  Off by default: the
+// one-wave step grid measured 1.3 % faster with ordinary launches inside the
+// captured graphs.
 bool pdl_enabled() {
     static const bool on = [] {
         const char* e = std::getenv("SWE_PDL");
-        return !(e && e[0] == '0');
+        return e && e[0] == '1';
     }();
     return on;
 }

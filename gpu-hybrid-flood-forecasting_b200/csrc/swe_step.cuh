@@ -398,9 +398,10 @@ struct PlanInputs {
 };
 
 // Issues the loads of a step's plan (every lane).  They are plain loads: the
-// previous step's writes are visible after griddepcontrol.wait, which the
-// kernel has passed, and a load that every warp of an SM makes is then merged
-// in the SM's L1 instead of reaching one L2 slice from every warp of the grid.
+// previous step's writes are visible to this grid (a kernel boundary, or
+// griddepcontrol.wait, which the kernel has passed, under programmatic
+// launch), and a load that every warp of an SM makes is then merged in the
+// SM's L1 instead of reaching one L2 slice from every warp of the grid.
 // The values are consumed later (plan_step), so the caller can start other
 // loads while these are in flight.
 __device__ __forceinline__ PlanInputs plan_fetch(const Control* c, int par) {
