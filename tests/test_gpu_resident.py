@@ -47,6 +47,26 @@ def test_resident_pieces_equal_one_advance(cuda_device, arith):
     assert n2 == total + 5 and t2 > t
 
 
+def test_prepared_graphs_give_the_same_steps(cuda_device):
+    """resident_prepare only captures: the prepared pieces run exactly as unprepared ones."""
+    s, init = _case("fast")
+    ref, t_ref, n_ref, led_ref = s.advance(init, 5 + 20 + 45, 0.0)
+    s.resident_load(init, 0.0)
+    s.resident_steps(5)
+    s.resident_prepare(20)  # an odd start: graphs of 20 steps from buffer 1
+    s.resident_prepare(0)
+    s.resident_steps(20)
+    s.resident_prepare(45)
+    s.resident_steps(45)
+    out = type(init)(*(torch.empty_like(t) for t in init))
+    t, n, led = s.resident_store(out)
+    assert (t, n) == (t_ref, n_ref) and led == led_ref
+    for a, b in zip(out, ref):
+        assert torch.equal(a, b)
+    with pytest.raises(ValueError):
+        s.resident_prepare(-1)
+
+
 def test_resident_run_is_ended_by_other_runs(cuda_device):
     s, init = _case("fast")
     out = type(init)(*(torch.empty_like(t) for t in init))
