@@ -477,6 +477,8 @@ int chunk_graph(swe_domain* d, const Plan& pl, int par, int len, cudaGraphExec_t
         slot = nullptr;
         return fail(SWE_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(err));
     }
+    // Uploaded now, ahead of its first launch.
+    SWE_CK(cudaGraphUpload(slot, d->cap_stream));
     *out = slot;
     return SWE_OK;
 }
