@@ -130,8 +130,8 @@ struct swe_domain {
     int64_t snap_cap = 0;  // floats
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t snap_ev = nullptr;
-    // CUDA graph of kChunk run-mode steps starting from ping buffer 0, and the
-    // inputs it was captured with (a change of any of them re-captures it).
+    // CUDA graphs of 1..kChunk run-mode steps from either ping buffer, and the
+    // inputs they were captured with (a change of any of them re-captures them).
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t chunk_graph[2][33] = {};  // [start buffer parity][steps 1..32]
     const LedgerSlot* chunk_graph_slots = nullptr;
@@ -420,8 +420,7 @@ int fold_ledger(swe_domain* d, int ncta, cudaStream_t st) {
     return SWE_OK;
 }
 
-// Steps per poll of the run driver and per captured step graph (even, so that
-// a graph always starts and ends on ping buffer 0).
+// Steps per poll of the run driver and at most per captured step graph.
 constexpr int kChunk = 32;
 
 // Run-mode launch of step k of a run (buffer parity k & 1).
