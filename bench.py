@@ -18,10 +18,11 @@ K step launches (whole 32-step CUDA graphs where K allows), bracketed by a
 barrier and a device synchronisation, timed with CUDA events on the launching
 stream.  ``value`` is cell-updates/s over those K steps.  The per-step working
 set is 134 MB (five input planes and three output planes of 16.8 MB), above the
-126 MB L2, so no flush is inserted.  ``e2e`` times ``B200ShallowWaterSolver.run``
+126 MB L2, so no flush is inserted.  ``e2e`` times ``B200ShallowWaterSolver.run_to_host``
 called with HOST (pinned NumPy-backed) state over a forecast window with six
 output times, the host->device copy of the state and the device->host copy of
-every recorded snapshot inside the timed region.
+every recorded snapshot inside the timed region (``run_to_host``).  The line
+also carries the same resident timing in exact arithmetic (``exact_arithmetic``).
 
 Multi-GPU: one process per GPU, each advancing its own replica of the domain
 (weak scaling, no collective in the timed region); ``value`` is the sum over
@@ -87,6 +88,7 @@ def _args():
     ap.add_argument("--training-members", type=int, default=16)
     ap.add_argument("--training-size", type=int, default=1024)
     ap.add_argument("--no-aux", action="store_true", help="skip the timing of the kernels around the step")
+    ap.add_argument("--exact-steps", type=int, default=200, help="steps of the exact-arithmetic leg (0: skip)")
     ap.add_argument("--aux-size", type=int, default=4096)
     ap.add_argument("--decompose", action="store_true",
                     help="also time the single domain split into row strips, one per GPU over NCCL (strong scaling)")
@@ -758,8 +760,41 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def _exact_leg(args, w, depth, dev) -> dict:
+    """The same resident step timing in exact arithmetic (the mode that is bit-identical
+    to the reference's float32 NumPy solver on its golden runs): W warm-up steps, then
+    ``--exact-steps`` steps between CUDA events."""
+    import torch
+
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver
+
+    solver = B200ShallowWaterSolver(w.bed, w.manning_n, w.domain_mask, **w.solver_kwargs(), arithmetic="exact",
+                                    device=dev)
+    state = solver.initial_state(depth_m=depth)
+    t_sim, _, _ = solver.advance_(state, args.spinup, 0.0)
+    solver.resident_load(state, t_sim)
+    solver.resident_steps(args.warmup)
+    solver.resident_prepare(args.exact_steps)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    torch.cuda._sleep(200_000)
+    e0.record(stream)
+    solver.resident_steps(args.exact_steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    solver.resident_store(state)
+    cells = w.bed.size
+    value = cells * args.exact_steps / (ms / 1e3)
+    peak, kind = _peaks()
+    return {"value": value, "unit": "cell-updates/s", "steps": args.exact_steps, "ms_per_step": ms / args.exact_steps,
+            "roofline_frac": BYTES_PER_CELL * value / 1e9 / peak, "peak_kind": kind,
+            "arith": "exact (IEEE-rounded float32, the reference's operation order)"}
+
+
 def _e2e(args, solver, state, t_sim, dev, world: int) -> dict:
-    """``B200ShallowWaterSolver.run`` with host state: a forecast window of about
+    """``B200ShallowWaterSolver.run_to_host`` with host state: a forecast window of about
     ``--e2e-steps`` steps with six output times; the state goes in from pinned
     host memory and every recorded snapshot comes back to pinned host memory
     inside the timed region."""
@@ -861,6 +896,7 @@ def run_b200(args, rank: int, world: int):
     window = t_sim - t_before
 
     e2e = None if args.no_e2e else _e2e(args, solver, state, t_sim, dev, world)
+    exact = _exact_leg(args, w, depth, dev) if (args.arith == "fast" and args.exact_steps > 0 and rank == 0) else None
     dec = _decomposed(args, dev, rank, world) if args.decompose else None
     ens = None
     if not args.no_ensemble:
@@ -908,6 +944,8 @@ def run_b200(args, rank: int, world: int):
     }
     if e2e:
         line["e2e"] = e2e
+    if exact:
+        line["exact_arithmetic"] = exact
     if par:
         line["parity"] = par
     if ens:
