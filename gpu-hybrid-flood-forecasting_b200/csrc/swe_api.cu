@@ -1110,6 +1110,14 @@ int swe_domain_create(const swe_domain_desc* desc, swe_domain_t* out) {
     dd.k.dry = (float)q.dry_tolerance;
     dd.k.dx = (float)q.dx;
     dd.k.dy = (float)q.dy;
+    {
+        // An exact power of two within float range: its reciprocal is exact too.
+        auto pow2 = [](float v) {
+            int e = 0;
+            return v > 0.f && std::frexp(v, &e) == 0.5f && e > -120 && e < 120;
+        };
+        dd.k.pow2 = pow2(dd.k.dx) && pow2(dd.k.dy) ? 1 : 0;
+    }
     dd.k.eps = (float)1.0e-12;
     dd.k.expo = (float)(7.0 / 3.0);
     dd.dx = q.dx;

@@ -43,6 +43,7 @@ struct Consts {
     float dx, dy;  // float(dx), float(dy)
     float eps;     // float(1e-12)   HLL denominator guard
     float expo;    // float(7/3)     Manning exponent
+    int pow2;      // 1: dx and dy are powers of two, so x / dx == x * (1 / dx) exactly
 };
 
 // Per-step float32 scalars: float(dt), float(dt*rate), float(dt*g).

@@ -101,6 +101,19 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
     const float rdx = 1.0f / k.dx, rdy = 1.0f / k.dy;
     const float2 rdx2 = splat(rdx), rdy2 = splat(rdy);
     const float2 nexpo2 = splat(-k.expo);
+    // Exact arithmetic divides by dx and dy as the reference does; when both are
+    // powers of two that is the multiplication by their (exact) reciprocals, the
+    // same correctly rounded result (a warp-uniform branch).
+    const bool pow2 = k.pow2 != 0;
+    const float2 rdxe = splat(__frcp_rn(k.dx)), rdye = splat(__frcp_rn(k.dy));
+    auto over_dx = [&](float2 a) {
+        if constexpr (A::kExact) return pow2 ? A::mul(a, rdxe) : A::div(a, dx2);
+        else return A::mul(a, rdxe);  // not used by the fast policy
+    };
+    auto over_dy = [&](float2 a) {
+        if constexpr (A::kExact) return pow2 ? A::mul(a, rdye) : A::div(a, dy2);
+        else return A::mul(a, rdye);
+    };
     const int nq = r1 - r0 + 2;  // rows r0-1 .. r1 pass through the ring
     const bool edge_strip = x0w + kWarp * 2 > d.cols;
     const int csize = valid.y ? 8 : (valid.x ? 4 : 0);
@@ -248,9 +261,9 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
         const float2 n2 = MASKED ? vabs(cur.nm) : cur.nm;
         float2 u0, u1, u2;
         if constexpr (A::kExact) {
-            u0 = A::sub(cur.h, A::mul(dt2, A::add(A::div(A::sub(x.r0, x.l0), dx2), A::div(A::sub(t0, b0), dy2))));
-            u1 = A::sub(cur.hu, A::mul(dt2, A::add(A::div(A::sub(x.r1, x.l1), dx2), A::div(A::sub(t1, b1), dy2))));
-            u2 = A::sub(cur.hv, A::mul(dt2, A::add(A::div(A::sub(x.r2, x.l2), dx2), A::div(A::sub(t2, b2), dy2))));
+            u0 = A::sub(cur.h, A::mul(dt2, A::add(over_dx(A::sub(x.r0, x.l0)), over_dy(A::sub(t0, b0)))));
+            u1 = A::sub(cur.hu, A::mul(dt2, A::add(over_dx(A::sub(x.r1, x.l1)), over_dy(A::sub(t1, b1)))));
+            u2 = A::sub(cur.hv, A::mul(dt2, A::add(over_dx(A::sub(x.r2, x.l2)), over_dy(A::sub(t2, b2)))));
         } else {
             u0 = A::fma(ndtdx2, A::sub(x.r0, x.l0), A::fma(ndtdy2, A::sub(t0, b0), cur.h));
             u1 = A::fma(ndtdx2, A::sub(x.r1, x.l1), A::fma(ndtdy2, A::sub(t1, b1), cur.hu));
@@ -292,7 +305,7 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
                 nc.hu = o.hu;
                 nc.hv = o.hv;
                 set_vel_t<M>(nc, kp);
-                inv = A::add(A::div(A::add(vabs(nc.u), w), dx2), A::div(A::add(vabs(nc.v), w), dy2));
+                inv = A::add(over_dx(A::add(vabs(nc.u), w)), over_dy(A::add(vabs(nc.v), w)));
             } else {
                 // The new momenta are zero wherever h <= dry, so 1/max(h, dry) gives the
                 // same velocities as the dry-cell rule of the reference.
