@@ -72,6 +72,17 @@ def _replay_backward(dom, x0: SWEState, dts: np.ndarray, t0: float, grad_out: SW
     return SWEState(*lam)
 
 
+_SIDE_STREAMS: dict = {}
+SIDE_STREAMS = 4  # concurrent member replays in an ensemble interval's backward
+
+
+def _side_streams(dev: torch.device) -> list:
+    key = (dev.index, SIDE_STREAMS)
+    if key not in _SIDE_STREAMS:
+        _SIDE_STREAMS[key] = [torch.cuda.Stream(dev) for _ in range(SIDE_STREAMS)]
+    return _SIDE_STREAMS[key]
+
+
 def _nan_if_short(state, t: float, target: float) -> None:
     if not t >= target - 1.0e-6:
         for x in state:
@@ -132,14 +143,29 @@ class EnsembleInterval(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, *grads):
+        # The members' replays are independent, so they run on a few side streams
+        # at once: a member's steps fill the GPU only between their starts and
+        # tails, which the other members' kernels fill in.
         t0, dts = ctx.meta
         x0 = ctx.saved_tensors
+        dev = x0[0].device
+        main = torch.cuda.current_stream(dev)
+        streams = _side_streams(dev)
         out = []
         for m, dom in enumerate(ctx.doms):
             xm = SWEState(*x0[3 * m:3 * m + 3])
             g = SWEState(*(torch.zeros_like(xm.h) if a is None else a for a in grads[3 * m:3 * m + 3]))
-            lam = _replay_backward(dom, xm, dts[m], t0, g)
+            s = streams[m % len(streams)]
+            s.wait_stream(main)
+            for t in (*xm, *g):
+                t.record_stream(s)  # made on the main stream, read on this one
+            with torch.cuda.stream(s):
+                lam = _replay_backward(dom, xm, dts[m], t0, g)
+            for t in lam:
+                t.record_stream(main)  # made on this stream, read on the main one
             out.extend(lam)
+        for s in streams:
+            main.wait_stream(s)
         return (None, None, None, None, *out)
 
 
