@@ -122,6 +122,13 @@ struct swe_domain {
     int64_t lpitch = 0;
     double* times64_dev = nullptr;  // float64 targets of advance_to
     float* next_scratch = nullptr;  // rollout backward: the output of a segment's last step
+    // Rollout backward's second segment buffer, its last-step output, and the
+    // stream that recomputes the next segment while the current one is reversed.
+    float* seg2 = nullptr;
+    int64_t seg2_cap = 0;  // floats
+    float* next_scratch2 = nullptr;
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t seg_ev[6] = {};  // start, recomputed[2], reversed[2], end
     double* corr_sums = nullptr;    // volume sums of the residual correction
     float* corr_prov = nullptr;     // provisional-depth plane of the correction
     unsigned* done_counter = nullptr;  // set by an ensemble: shared completion counter
@@ -579,6 +586,11 @@ void free_domain(swe_domain* d) {
     for (int q = 0; q < 3; ++q) cudaFree(d->lupd[q]);
     cudaFree(d->times64_dev);
     cudaFree(d->next_scratch);
+    cudaFree(d->next_scratch2);
+    cudaFree(d->seg2);
+    for (cudaEvent_t e : d->seg_ev)
+        if (e) cudaEventDestroy(e);
+    if (d->aux_stream) cudaStreamDestroy(d->aux_stream);
     cudaFree(d->corr_sums);
     cudaFree(d->corr_prov);
     for (int i = 0; i < 2; ++i) {
@@ -1802,28 +1814,64 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
         for (int f = 0; f < 3; ++f)
             SWE_CK(cudaMemset2DAsync(lam[f], sizeof(float) * lam_pitch, 0, sizeof(float) * cols, rows, st));
     const int nseg = n_steps > 0 ? (n_steps + ckpt_every - 1) / ckpt_every : 0;
-    for (int sgi = nseg - 1; sgi >= 0; --sgi) {
+    // Two segment buffers: the caller's `seg` and one of the domain's.  Segment
+    // s-1 is recomputed on the domain's auxiliary stream while segment s is
+    // reversed on the caller's stream (events order the reuse of a buffer), so
+    // the recomputation overlaps the reverse steps instead of following them.
+    const int64_t seg_floats = (int64_t)ckpt_every * 3 * plane;
+    if (nseg > 1 && d->seg2_cap < seg_floats) {
+        if (d->seg2) cudaFree(d->seg2);
+        d->seg2 = nullptr;
+        d->seg2_cap = 0;
+        SWE_CK(cudaMalloc(&d->seg2, sizeof(float) * (size_t)seg_floats));
+        d->seg2_cap = seg_floats;
+    }
+    if (!d->next_scratch2) SWE_CK(cudaMalloc(&d->next_scratch2, sizeof(float) * 3 * (size_t)plane));
+    if (!d->aux_stream) SWE_CK(cudaStreamCreateWithFlags(&d->aux_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : d->seg_ev)
+        if (!e) SWE_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaStream_t aux = d->aux_stream;
+    cudaEvent_t ev_start = d->seg_ev[0], ev_end = d->seg_ev[5];
+    cudaEvent_t* ev_rec = d->seg_ev + 1;   // segment buffer b recomputed
+    cudaEvent_t* ev_used = d->seg_ev + 3;  // segment buffer b reversed (free again)
+    float* segbuf[2] = {seg, d->seg2};
+    float* nxtbuf[2] = {d->next_scratch, d->next_scratch2};
+    // Recompute segment sgi's states U_k0 .. U_{k1-1} into segbuf[b] and U_{k1},
+    // the output of its last step, into nxtbuf[b] (so that every reverse step can
+    // rebuild its cell updates from its own output), on the auxiliary stream.
+    auto recompute = [&](int sgi, int b) -> int {
         const int k0 = sgi * ckpt_every;
         const int k1 = std::min(k0 + ckpt_every, n_steps);
-        // Recompute the segment's states U_k0 .. U_{k1-1} into seg[0 .. k1-k0-1].
-        SWE_CK(cudaMemcpyAsync(seg, ckpt + (int64_t)sgi * 3 * plane, sizeof(float) * 3 * plane,
-                               cudaMemcpyDeviceToDevice, st));
-        for (int k = k0; k < k1 - 1; ++k) {
-            const float* a = seg + (int64_t)(k - k0) * 3 * plane;
-            float* b = seg + (int64_t)(k + 1 - k0) * 3 * plane;
-            rc = swe_step(d, a, a + plane, a + 2 * plane, cols, b, b + plane, b + 2 * plane, cols,
-                          dts ? dts[k] : dt, step_time(k, dt, t0, dts), stream);
+        float* sb = segbuf[b];
+        SWE_CK(cudaMemcpyAsync(sb, ckpt + (int64_t)sgi * 3 * plane, sizeof(float) * 3 * plane,
+                               cudaMemcpyDeviceToDevice, aux));
+        for (int k = k0; k < k1; ++k) {
+            const float* a = sb + (int64_t)(k - k0) * 3 * plane;
+            float* o = k + 1 < k1 ? sb + (int64_t)(k + 1 - k0) * 3 * plane : nxtbuf[b];
+            const int src = swe_step(d, a, a + plane, a + 2 * plane, cols, o, o + plane, o + 2 * plane, cols,
+                                     dts ? dts[k] : dt, step_time(k, dt, t0, dts), aux);
+            if (src) return src;
+        }
+        SWE_CK(cudaEventRecord(ev_rec[b], aux));
+        return SWE_OK;
+    };
+    SWE_CK(cudaEventRecord(ev_start, st));  // the checkpoints and lam are ready on the caller's stream
+    SWE_CK(cudaStreamWaitEvent(aux, ev_start, 0));
+    if (nseg > 0) {
+        rc = recompute(nseg - 1, 0);
+        if (rc) return rc;
+    }
+    for (int i = 0; i < nseg; ++i) {
+        const int sgi = nseg - 1 - i, b = i & 1;
+        const int k0 = sgi * ckpt_every;
+        const int k1 = std::min(k0 + ckpt_every, n_steps);
+        if (sgi > 0) {
+            if (i >= 1) SWE_CK(cudaStreamWaitEvent(aux, ev_used[b ^ 1], 0));  // buffer b^1 reversed
+            rc = recompute(sgi - 1, b ^ 1);
             if (rc) return rc;
         }
-        // U_{k1}, the output of the segment's last step, so that every reverse step
-        // can rebuild its cell updates from its own output.
-        {
-            const float* a = seg + (int64_t)(k1 - 1 - k0) * 3 * plane;
-            rc = swe_step(d, a, a + plane, a + 2 * plane, cols, d->next_scratch, d->next_scratch + plane,
-                          d->next_scratch + 2 * plane, cols, dts ? dts[k1 - 1] : dt, step_time(k1 - 1, dt, t0, dts),
-                          stream);
-            if (rc) return rc;
-        }
+        SWE_CK(cudaStreamWaitEvent(st, ev_rec[b], 0));
+        const float* sb = segbuf[b];
         for (int k = k1 - 1; k >= k0; --k) {
             // dL/dU_{k+1} is in buffer `cur`; dL/dU_k goes to the other one (the fused
             // reverse step reads its neighbours' lam while it writes lam_out).
@@ -1834,15 +1882,18 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
                 gauge_inject_kernel<<<(n_gauges + 127) / 128, 128, 0, st>>>(
                     src[0], sp, cols, gauge_index, n_gauges, grad_obs + (int64_t)((k + 1) / obs_every - 1) * n_gauges);
             }
-            const float* a = seg + (int64_t)(k - k0) * 3 * plane;
-            const float* nx = k + 1 < k1 ? seg + (int64_t)(k + 1 - k0) * 3 * plane : d->next_scratch;
+            const float* a = sb + (int64_t)(k - k0) * 3 * plane;
+            const float* nx = k + 1 < k1 ? sb + (int64_t)(k + 1 - k0) * 3 * plane : nxtbuf[b];
             rc = adjoint_step_impl(d, a, a + plane, a + 2 * plane, cols, nx, cols, plane, src[0], src[1], src[2], sp,
                                    dst[0], dst[1], dst[2], dp, grad_n2, grad_rain_scale, dts ? dts[k] : dt,
                                    step_time(k, dt, t0, dts), st);
             if (rc) return rc;
             cur ^= 1;
         }
+        SWE_CK(cudaEventRecord(ev_used[b], st));
     }
+    SWE_CK(cudaEventRecord(ev_end, aux));  // every recomputation is behind the caller's stream
+    SWE_CK(cudaStreamWaitEvent(st, ev_end, 0));
     if (cur) {  // the result is in the alternate buffers: copy it to the caller's lam planes
         for (int f = 0; f < 3; ++f) {
             rc = copy_plane(lam[f], lam_pitch, alt[f], d->lpitch, rows, cols, st);
