@@ -211,8 +211,12 @@ int swe_rollout_forward(swe_domain_t d, float *h, float *hu, float *hv, int64_t 
  * lam_hv), and ADDS dL/d(n^2) into grad_n2 and dL/d(rain scale) into
  * *grad_rain_scale.  lam_in = 1: the lam planes hold dL/dU_{n_steps} on entry
  * (a loss on the final state); 0: they start at zero.  Each segment of
- * ckpt_every steps is recomputed from its checkpoint into seg (device,
- * ckpt_every*3*rows*cols floats) and reversed step by step. */
+ * ckpt_every steps is recomputed from its checkpoint and reversed step by
+ * step; seg (device, ckpt_every*3*rows*cols floats) and a second buffer of the
+ * domain's hold two segments, so that the next segment is recomputed on a
+ * stream of the domain's own while the current one is reversed on `stream`.
+ * That stream waits for `stream`'s earlier work and `stream` waits for it
+ * before the call's last work: callers see only `stream`. */
 int swe_rollout_backward(swe_domain_t d, const float *ckpt, int32_t ckpt_every, int32_t n_steps,
                          double dt, double t0, const double *dts, const int64_t *gauge_index,
                          int32_t n_gauges, int32_t obs_every, const float *grad_obs, float *lam_h,
