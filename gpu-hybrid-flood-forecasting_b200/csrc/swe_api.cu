@@ -634,7 +634,7 @@ struct swe_ensemble {
     std::vector<swe_domain*> doms;
     int arith = SWE_ARITH_FAST;
     bool masked = false;
-    int rows_per_warp = 128;  // a good default on the 64-member mix; B200Ensemble.autotune searches 32-256
+    int rows_per_warp = 128;  // provisional: swe_ensemble_create sets ens_auto_rows (B200Ensemble.autotune measures)
     int sms = 148;
     MemberDev* members_dev = nullptr;
     int members_cap = 0;
@@ -701,6 +701,33 @@ int ens_occupancy(const swe_ensemble* e) {
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kThreads, 0) != cudaSuccess || n < 1) n = 1;
     return n;
+}
+
+// Default rows per warp: the step of a batch that fits the persistent grid in
+// one round takes about as long as its longest march, so the default is the
+// smallest march (at least 32 rows) whose work items all fit in one round of
+// the grid; when even 1024-row marches need more than one round, 256.
+int ens_occupancy(const swe_ensemble* e);
+int ens_auto_rows(const swe_ensemble* e) {
+    const int wpb = kThreads / kWarp;
+    const int64_t slots = (int64_t)ens_occupancy(e) * e->sms;
+    auto items = [&](int R) {
+        int64_t n = 0;
+        for (const swe_domain* d : e->doms) {
+            const int64_t nstrips = (d->dd.cols + 2 * kWarp - 1) / (2 * kWarp);
+            const int64_t chunks = (d->dd.rows + R - 1) / R;
+            n += (chunks * nstrips + wpb - 1) / wpb;
+        }
+        return n;
+    };
+    if (items(1024) > slots) return 256;
+    int lo = 32, hi = 1024;  // items(hi) <= slots; items is non-increasing in R
+    if (items(lo) <= slots) return lo;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (items(mid) <= slots) hi = mid; else lo = mid;
+    }
+    return hi;
 }
 
 // Member table and work list for the current rows-per-warp.
@@ -1928,7 +1955,14 @@ int swe_ensemble_create(const swe_domain_desc* descs, int32_t n_members, swe_ens
         e->masked = e->masked || d->masked;
         e->sms = d->sms;
     }
-    const int rc = ens_rebuild(e);
+    int rc = ens_rebuild(e);
+    if (!rc && !std::getenv("SWE_ENSEMBLE_ROWS")) {
+        const int R = ens_auto_rows(e);
+        if (R != e->rows_per_warp) {
+            e->rows_per_warp = R;
+            rc = ens_rebuild(e);
+        }
+    }
     if (rc) {
         free_ensemble(e);
         return rc;
@@ -1936,6 +1970,8 @@ int swe_ensemble_create(const swe_domain_desc* descs, int32_t n_members, swe_ens
     *out = e;
     return SWE_OK;
 }
+
+int32_t swe_ensemble_rows_per_warp(swe_ensemble_t e) { return e ? e->rows_per_warp : -1; }
 
 int swe_ensemble_destroy(swe_ensemble_t e) {
     if (!e) return SWE_OK;

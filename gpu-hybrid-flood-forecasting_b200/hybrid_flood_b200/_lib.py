@@ -57,6 +57,7 @@ EXPORTS = (
     "swe_ensemble_destroy",
     "swe_ensemble_size",
     "swe_ensemble_set_rows_per_warp",
+    "swe_ensemble_rows_per_warp",
     "swe_ensemble_advance",
     "swe_ensemble_advance_to",
     "swe_ensemble_member",
@@ -188,6 +189,7 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_ensemble_destroy": (ctypes.c_int, [_vp]),
         "swe_ensemble_size": (ctypes.c_int, [_vp]),
         "swe_ensemble_set_rows_per_warp": (ctypes.c_int, [_vp, _i32]),
+        "swe_ensemble_rows_per_warp": (_i32, [_vp]),
         "swe_ensemble_advance": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp,
                                                 ctypes.POINTER(RunResult), _vp]),
         "swe_ensemble_advance_to": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f64, _i32, _vp,

@@ -106,7 +106,7 @@ class B200Ensemble:
         self.shapes = [tuple(m["bed"].shape) for m in members]
         self.masks = [torch.as_tensor(m["domain_mask"]).to(device=self.device, dtype=torch.bool) for m in members]
         self.arithmetic = arithmetic
-        self.rows_per_warp = 128
+        self.rows_per_warp = int(self._lib.swe_ensemble_rows_per_warp(handle))  # the library's one-round default
         self.dry_tolerances = [float(m.get("dry_tolerance_m", 1.0e-4)) for m in members]
         self.beds = [m["bed"].detach().cpu().numpy().astype(np.float32) if isinstance(m["bed"], torch.Tensor)
                      else np.asarray(m["bed"], dtype=np.float32) for m in members]

@@ -291,8 +291,13 @@ int swe_ensemble_create(const swe_domain_desc *descs, int32_t n_members, swe_ens
 int swe_ensemble_destroy(swe_ensemble_t e);
 int swe_ensemble_size(swe_ensemble_t e);
 
-/* Rows each warp marches per work item (the tuning knob of the work list; default 64). */
+/* Rows each warp marches per work item (the tuning knob of the work list).
+ * The default, chosen at creation, is the smallest march of at least 32 rows
+ * whose work items fit the persistent grid in one round (256 when none does);
+ * SWE_ENSEMBLE_ROWS overrides it.  swe_ensemble_rows_per_warp returns the
+ * current value (-1 for a null handle). */
 int swe_ensemble_set_rows_per_warp(swe_ensemble_t e, int32_t rows_per_warp);
+int32_t swe_ensemble_rows_per_warp(swe_ensemble_t e);
 
 /* Advance every member IN PLACE by n_steps of its own CFL dt, starting at
  * start_s[m] (NULL = 0).  h/hu/hv/pitch are arrays of n_members device
