@@ -1884,20 +1884,29 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
     };
     SWE_CK(cudaEventRecord(ev_start, st));  // the checkpoints and lam are ready on the caller's stream
     SWE_CK(cudaStreamWaitEvent(aux, ev_start, 0));
+    // On every return the caller's stream waits for the auxiliary stream, so no
+    // recomputation is left running into the caller's buffers after an error.
+    auto join = [&](int status) {
+        cudaEventRecord(ev_end, aux);
+        cudaStreamWaitEvent(st, ev_end, 0);
+        return status;
+    };
     if (nseg > 0) {
         rc = recompute(nseg - 1, 0);
-        if (rc) return rc;
+        if (rc) return join(rc);
     }
     for (int i = 0; i < nseg; ++i) {
         const int sgi = nseg - 1 - i, b = i & 1;
         const int k0 = sgi * ckpt_every;
         const int k1 = std::min(k0 + ckpt_every, n_steps);
         if (sgi > 0) {
-            if (i >= 1) SWE_CK(cudaStreamWaitEvent(aux, ev_used[b ^ 1], 0));  // buffer b^1 reversed
+            if (i >= 1 && cudaStreamWaitEvent(aux, ev_used[b ^ 1], 0) != cudaSuccess)  // buffer b^1 reversed
+                return join(fail(SWE_ERR_CUDA, "cudaStreamWaitEvent failed"));
             rc = recompute(sgi - 1, b ^ 1);
-            if (rc) return rc;
+            if (rc) return join(rc);
         }
-        SWE_CK(cudaStreamWaitEvent(st, ev_rec[b], 0));
+        if (cudaStreamWaitEvent(st, ev_rec[b], 0) != cudaSuccess)
+            return join(fail(SWE_ERR_CUDA, "cudaStreamWaitEvent failed"));
         const float* sb = segbuf[b];
         for (int k = k1 - 1; k >= k0; --k) {
             // dL/dU_{k+1} is in buffer `cur`; dL/dU_k goes to the other one (the fused
@@ -1914,13 +1923,12 @@ int swe_rollout_backward(swe_domain_t d, const float* ckpt, int32_t ckpt_every, 
             rc = adjoint_step_impl(d, a, a + plane, a + 2 * plane, cols, nx, cols, plane, src[0], src[1], src[2], sp,
                                    dst[0], dst[1], dst[2], dp, grad_n2, grad_rain_scale, dts ? dts[k] : dt,
                                    step_time(k, dt, t0, dts), st);
-            if (rc) return rc;
+            if (rc) return join(rc);
             cur ^= 1;
         }
-        SWE_CK(cudaEventRecord(ev_used[b], st));
+        if (cudaEventRecord(ev_used[b], st) != cudaSuccess) return join(fail(SWE_ERR_CUDA, "cudaEventRecord failed"));
     }
-    SWE_CK(cudaEventRecord(ev_end, aux));  // every recomputation is behind the caller's stream
-    SWE_CK(cudaStreamWaitEvent(st, ev_end, 0));
+    join(SWE_OK);  // every recomputation is behind the caller's stream
     if (cur) {  // the result is in the alternate buffers: copy it to the caller's lam planes
         for (int f = 0; f < 3; ++f) {
             rc = copy_plane(lam[f], lam_pitch, alt[f], d->lpitch, rows, cols, st);
