@@ -149,3 +149,26 @@ def test_ensemble_ledger_drift_is_the_float32_schemes(cuda_device):
           f"float64 oracle {drift['f64']:.3g}")
     assert drift["f64"] < 1e-10
     assert errs[m] <= 1e-6 or errs[m] <= 3.0 * drift["f32"], (errs[m], drift)
+
+
+def test_default_rows_per_warp_fits_one_round(cuda_device, monkeypatch):
+    """Without tuning an ensemble marches the fewest rows (at least 32) whose work
+    items fit the persistent grid (4 CTAs of 4 warps per SM) in one round."""
+    from hybrid_flood_b200.ensemble import B200Ensemble
+    from hybrid_flood_b200.workloads import as_member, urban
+
+    monkeypatch.delenv("SWE_ENSEMBLE_ROWS", raising=False)
+    sms = torch.cuda.get_device_properties(cuda_device).multi_processor_count
+    slots = 4 * sms
+
+    def items(shapes, R):
+        return sum(-(-(-(-r // R) * -(-c // 64)) // 4) for r, c in shapes)
+
+    w = urban(1024, 1024, seed=3)
+    shapes = [w.shape] * 16
+    ens = B200Ensemble([as_member(w)] * 16, arithmetic="fast")
+    R = ens.rows_per_warp
+    assert R >= 32 and items(shapes, R) <= slots
+    assert R == 32 or items(shapes, R - 1) > slots
+    small = urban(96, 128, seed=4)
+    assert B200Ensemble([as_member(small)] * 3, arithmetic="fast").rows_per_warp == 32
