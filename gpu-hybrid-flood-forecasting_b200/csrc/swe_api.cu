@@ -379,13 +379,24 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
         SWE_CK(cudaMalloc(&d->times_dev, sizeof(float) * (size_t)n_times));
         d->times_cap = n_times;
     }
-    SWE_CK(cudaMemcpyAsync(d->times_dev, times_host, sizeof(float) * (size_t)n_times,
-                           cudaMemcpyHostToDevice, st));
+    // Output times (up to kInlineTimes: every advance, ensemble interval and
+    // ordinary run) travel with the control block's launch parameters; longer
+    // output lists are copied.
+    static_assert(kInlineTimes <= 128, "one thread of control_init_kernel per inline time");
+    RunTargets tg{};
+    if (n_times <= kInlineTimes) {
+        tg.n = n_times;
+        tg.times = d->times_dev;
+        for (int i = 0; i < n_times; ++i) tg.t[i] = times_host[i];
+    } else {
+        SWE_CK(cudaMemcpyAsync(d->times_dev, times_host, sizeof(float) * (size_t)n_times,
+                               cudaMemcpyHostToDevice, st));
+    }
     if (times64_host) {
         if (n_times > 2) return fail(SWE_ERR_INVALID, "float64 targets support one interval");
         if (!d->times64_dev) SWE_CK(cudaMalloc(&d->times64_dev, 2 * sizeof(double)));
-        SWE_CK(cudaMemcpyAsync(d->times64_dev, times64_host, sizeof(double) * (size_t)n_times,
-                               cudaMemcpyHostToDevice, st));
+        tg.times64 = d->times64_dev;
+        for (int i = 0; i < n_times; ++i) tg.t64[i] = times64_host[i];
     }
     if (out_h) {
         float* outs[3] = {out_h, out_hu, out_hv};
@@ -409,8 +420,10 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
     c0.out_hu = out_hu;
     c0.out_hv = out_hv;
     c0.out_plane = (int64_t)rows * cols;
-    // Pageable source: the copy is staged before cudaMemcpyAsync returns.
-    SWE_CK(cudaMemcpyAsync(d->ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, st));
+    ControlHeadImage img;
+    std::memcpy(&img, &c0, sizeof(img));
+    control_init_kernel<<<1, 128, 0, st>>>(d->ctl, img, tg);
+    SWE_CK(cudaGetLastError());
     StateView v0{d->ping[0][0], d->ping[0][1], d->ping[0][2], d->ppitch};
     launch_reduce(d, v0, d->ctl, st);
     SWE_CK(cudaGetLastError());
@@ -823,15 +836,18 @@ int ens_graph(swe_ensemble* e, int K) {
 int ens_collect(swe_ensemble* e, float* const* h, float* const* hu, float* const* hv, const int64_t* pitch,
                 swe_run_result* results, cudaStream_t st, bool need_target) {
     const int n = (int)e->doms.size();
+    // Every member's ledger fold and control-block read are queued first and
+    // waited for once; the final states are then copied out in stream order.
     for (int m = 0; m < n; ++m) {
-        const int rc = fold_ledger(e->doms[m], e->member_ncta[m], st);
+        swe_domain* d = e->doms[m];
+        const int rc = fold_ledger(d, e->member_ncta[m], st);
         if (rc) return rc;
+        SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl, kControlHead, cudaMemcpyDeviceToHost, st));
     }
     SWE_CK(cudaStreamSynchronize(st));
     int status = SWE_OK;
     for (int m = 0; m < n; ++m) {
         swe_domain* d = e->doms[m];
-        SWE_CK(cudaMemcpy(&d->ctl_host[0], d->ctl, kControlHead, cudaMemcpyDeviceToHost));
         const Control& c = d->ctl_host[0];
         swe_run_result& r = results[m];
         r.final_time_s = c.t;
@@ -849,7 +865,6 @@ int ens_collect(swe_ensemble* e, float* const* h, float* const* hu, float* const
             if (rc) return rc;
         }
     }
-    SWE_CK(cudaStreamSynchronize(st));
     if (status == SWE_ERR_NONFINITE) return fail(SWE_ERR_NONFINITE, "non-finite values reached a member's CFL reduction");
     if (status == SWE_ERR_MAX_STEPS) return fail(status, "an ensemble member did not reach its target time");
     if (status) return fail(status, "an ensemble member stopped with an error status");
@@ -1351,9 +1366,7 @@ int swe_max_inverse_dt(swe_domain_t d, const float* h, const float* hu, const fl
     rc = ensure_parts(d, reduce_blocks(d));
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    Control c0;
-    std::memset(&c0, 0, sizeof(c0));
-    SWE_CK(cudaMemcpyAsync(d->ctl_scratch, &c0, sizeof(Control), cudaMemcpyHostToDevice, st));
+    SWE_CK(cudaMemsetAsync(d->ctl_scratch, 0, sizeof(Control), st));
     launch_reduce(d, StateView{h, hu, hv, pitch}, d->ctl_scratch, st);
     SWE_CK(cudaGetLastError());
     SWE_CK(cudaMemcpyAsync(&d->ctl_host[0], d->ctl_scratch, kControlHead, cudaMemcpyDeviceToHost, st));
@@ -2128,6 +2141,46 @@ int swe_ensemble_last_step_time(swe_ensemble_t e, double* ms, int64_t* steps) {
 }
 
 int64_t swe_ensemble_last_launch_count(swe_ensemble_t e) { return e ? e->launches : -1; }
+
+int swe_ensemble_network_features(swe_ensemble_t e, float* const* h, float* const* hu, float* const* hv,
+                                  const int64_t* pitch, int32_t layout, const float* mean, const float* stddev,
+                                  const float* rain_features, const float* const* terrain,
+                                  const float* const* roughness, void* out, int64_t out_member_stride,
+                                  int32_t out_bf16, void* stream) {
+    if (!e || !h || !hu || !hv || !pitch || !mean || !stddev || !rain_features || !out)
+        return fail(SWE_ERR_INVALID, "null argument");
+    if (out_member_stride < 0) return fail(SWE_ERR_INVALID, "out_member_stride must be >= 0");
+    const size_t esz = out_bf16 ? 2 : 4;
+    for (int m = 0; m < (int)e->doms.size(); ++m) {
+        void* om = static_cast<char*>(out) + (size_t)m * (size_t)out_member_stride * esz;
+        const int rc = swe_network_features(e->doms[m], h[m], hu[m], hv[m], pitch[m], layout, mean + 5 * m,
+                                            stddev + 5 * m, rain_features[m], terrain ? terrain[m] : nullptr,
+                                            roughness ? roughness[m] : nullptr, om, out_bf16, stream);
+        if (rc) return rc;
+    }
+    return SWE_OK;
+}
+
+int swe_ensemble_apply_correction(swe_ensemble_t e, float* const* h, float* const* hu, float* const* hv,
+                                  const int64_t* pitch, const void* residual, int32_t residual_bf16,
+                                  int64_t res_stride_member, int64_t res_stride_row, int64_t res_stride_col,
+                                  int64_t res_stride_channel, int32_t res_channels, const float* clip_limits,
+                                  double relaxation, float* const* h_out, float* const* hu_out,
+                                  float* const* hv_out, const int64_t* out_pitch, void* stream) {
+    if (!e || !h || !hu || !hv || !pitch || !residual || !h_out || !hu_out || !hv_out || !out_pitch)
+        return fail(SWE_ERR_INVALID, "null argument");
+    if (res_channels != 1 && res_channels != 3) return fail(SWE_ERR_INVALID, "residual must have 1 or 3 channels");
+    const size_t esz = residual_bf16 ? 2 : 4;
+    for (int m = 0; m < (int)e->doms.size(); ++m) {
+        const void* rm = static_cast<const char*>(residual) + (int64_t)m * res_stride_member * (int64_t)esz;
+        const int rc = swe_apply_correction(e->doms[m], h[m], hu[m], hv[m], pitch[m], rm, residual_bf16,
+                                            res_stride_row, res_stride_col, res_stride_channel, res_channels,
+                                            clip_limits ? clip_limits + (size_t)res_channels * m : nullptr,
+                                            relaxation, h_out[m], hu_out[m], hv_out[m], out_pitch[m], stream);
+        if (rc) return rc;
+    }
+    return SWE_OK;
+}
 
 
 int swe_max_inverse_dt_noalloc(const float* h, const float* hu, const float* hv, int64_t pitch,

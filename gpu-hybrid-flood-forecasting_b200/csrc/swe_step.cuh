@@ -146,6 +146,37 @@ struct Control {
 // Bytes of the control block the host reads back (everything before the maxima).
 constexpr size_t kControlHead = offsetof(Control, maxk);
 
+// A run's control block written from launch parameters: the head as the host
+// built it, the stripe maxima zeroed and up to two target times.  Parameters
+// are captured when the launch is queued, so the host needs no staging buffer,
+// and the queue never waits for the stream as a copy from pageable host memory
+// may.
+struct ControlHeadImage {
+    unsigned long long w[kControlHead / 8];
+};
+static_assert(kControlHead % 8 == 0 && sizeof(ControlHeadImage) <= 2048, "control head must fit the launch parameters");
+
+constexpr int kInlineTimes = 64;  // output times carried in the launch parameters
+
+struct RunTargets {
+    int n;              // entries of t (and of t64, at most 2, when times64 is set) written
+    float t[kInlineTimes];
+    double t64[2];
+    float* times;       // device arrays receiving them (times64 may be null)
+    double* times64;
+};
+
+__global__ void control_init_kernel(Control* ctl, const ControlHeadImage head, const RunTargets tg) {
+    auto* dst = reinterpret_cast<unsigned long long*>(ctl);
+    for (int i = threadIdx.x; i < (int)(kControlHead / 8); i += blockDim.x) dst[i] = head.w[i];
+    unsigned long long* mk = &ctl->maxk[0][0];
+    for (int i = threadIdx.x; i < 2 * kMaxStripes * kStripeWords; i += blockDim.x) mk[i] = 0ull;
+    if ((int)threadIdx.x < tg.n) {
+        tg.times[threadIdx.x] = tg.t[threadIdx.x];
+        if (tg.times64 && threadIdx.x < 2) tg.times64[threadIdx.x] = tg.t64[threadIdx.x];
+    }
+}
+
 struct Partial {
     float maxinv;
     double vol, rain, outflow, clip, mask;

@@ -64,6 +64,8 @@ EXPORTS = (
     "swe_ensemble_set_timing",
     "swe_ensemble_last_step_time",
     "swe_ensemble_last_launch_count",
+    "swe_ensemble_network_features",
+    "swe_ensemble_apply_correction",
     "swe_strip_create",
     "swe_strip_layout",
     "swe_strips_advance",
@@ -198,6 +200,10 @@ def load(path: pathlib.Path | None = None) -> ctypes.CDLL:
         "swe_ensemble_set_timing": (ctypes.c_int, [_vp, _i32]),
         "swe_ensemble_last_step_time": (ctypes.c_int, [_vp, ctypes.POINTER(_f64), ctypes.POINTER(_i64)]),
         "swe_ensemble_last_launch_count": (ctypes.c_int64, [_vp]),
+        "swe_ensemble_network_features": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp,
+                                                         _vp, _i64, _i32, _vp]),
+        "swe_ensemble_apply_correction": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i32, _i64, _i64, _i64,
+                                                         _i64, _i32, _vp, _f64, _vp, _vp, _vp, _vp, _vp]),
         "swe_strip_create": (ctypes.c_int, [ctypes.POINTER(DomainDesc), _i32, _i32, ctypes.POINTER(_vp)]),
         "swe_strip_layout": (ctypes.c_int, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
         "swe_strips_advance": (ctypes.c_int, [_vp, _i32, _vp, _vp, _vp, _vp, _i32, _f64, ctypes.POINTER(RunResult),

@@ -368,6 +368,112 @@ def ensemble_domains(ensemble) -> list[_Domain]:
     return out
 
 
+def _ptrs(tensors) -> ctypes.Array:
+    return (ctypes.c_void_p * len(tensors))(*[None if t is None else t.data_ptr() for t in tensors])
+
+
+def _pitches(states) -> ctypes.Array:
+    return (ctypes.c_int64 * len(states))(*[int(s.h.stride(0)) for s in states])
+
+
+def ensemble_network_features(ensemble, states, hybrid_inputs, time_s: float, *, layout: str = "state5",
+                              out: torch.Tensor, doms=None, planes=None) -> torch.Tensor:
+    """:func:`network_features` of every member of ``ensemble`` into ``out``
+    (``[M, rows, cols, C]`` channels-last, contiguous) in one library call.
+
+    ``hybrid_inputs``: one :class:`HybridInputs` or one per member; ``planes``:
+    per member ``(terrain, roughness)`` device planes (``reference6``).
+    """
+    if layout not in LAYOUTS:
+        raise ValueError(f"unknown feature layout {layout!r}; choose one of {sorted(LAYOUTS)}")
+    M = len(ensemble)
+    doms = ensemble_domains(ensemble) if doms is None else doms
+    his = [hybrid_inputs] * M if isinstance(hybrid_inputs, HybridInputs) else list(hybrid_inputs)
+    if len(his) != M or len(states) != M:
+        raise ValueError(f"expected {M} states and one HybridInputs or {M} of them")
+    if any(d.shape != doms[0].shape for d in doms):
+        raise ValueError("ensemble_network_features needs members of one grid shape")
+    states = [_check_state(st, d) for st, d in zip(states, doms)]
+    code, C = LAYOUTS[layout]
+    H, W = doms[0].shape
+    if (out.dtype not in (torch.float32, torch.bfloat16) or not out.is_contiguous() or out.device != ensemble.device
+            or tuple(out.shape) != (M, H, W, C)):
+        raise ValueError(f"out must be a contiguous [{M}, {H}, {W}, {C}] float32 or bfloat16 tensor on the device")
+    nstat = 3 if layout == "reference6" else 5
+    stats = np.zeros((2, M, 5), np.float32)
+    stats[1] = 1.0
+    for m, hi in enumerate(his):
+        stats[0, m, :nstat] = _host_f32(hi.state_mean, nstat, "state_mean")
+        stats[1, m, :nstat] = _host_f32(hi.state_std, nstat, "state_std")
+    rain = np.array([rain_feature(d, hi, time_s, layout) for d, hi in zip(doms, his)], np.float32)
+    if layout == "reference6":
+        if planes is None:
+            planes = [(_dev_plane(hi.terrain_standardized, d), _dev_plane(hi.roughness_standardized, d))
+                      for hi, d in zip(his, doms)]
+        terrain, rough = _ptrs([p[0] for p in planes]), _ptrs([p[1] for p in planes])
+    else:
+        terrain = rough = None
+    with torch.cuda.device(ensemble.device):
+        rc = ensemble._lib.swe_ensemble_network_features(
+            ensemble._handle, _ptrs([st.h for st in states]), _ptrs([st.hu for st in states]),
+            _ptrs([st.hv for st in states]), _pitches(states), code, stats[0].ctypes.data, stats[1].ctypes.data,
+            rain.ctypes.data, terrain, rough, _ptr(out), H * W * C, 1 if out.dtype == torch.bfloat16 else 0,
+            _stream(ensemble.device))
+    _lib.check(rc, "ensemble_network_features")
+    return out
+
+
+def ensemble_apply_correction(ensemble, predicted, residual: torch.Tensor, *, correction_relaxation: float,
+                              clip_limits=None, out=None, doms=None) -> list[SWEState]:
+    """:func:`apply_residual_correction` of every member in one library call.
+
+    ``residual``: ``[M, C, rows, cols]`` (the corrector's NCHW output, any
+    strides) or ``[M, rows, cols, C]``, float32 or bfloat16, read in place;
+    ``clip_limits``: ``None`` or one limit array per member; ``out`` may alias
+    ``predicted``.
+    """
+    M = len(ensemble)
+    doms = ensemble_domains(ensemble) if doms is None else doms
+    if any(d.shape != doms[0].shape for d in doms):
+        raise ValueError("ensemble_apply_correction needs members of one grid shape")
+    if len(predicted) != M:
+        raise ValueError(f"expected {M} predicted states")
+    predicted = [_check_state(st, d) for st, d in zip(predicted, doms)]
+    H, W = doms[0].shape
+    r = residual
+    if r.dim() != 4 or r.shape[0] != M:
+        raise ValueError(f"residual must be [{M}, C, rows, cols] or [{M}, rows, cols, C]")
+    if tuple(r.shape[2:]) == (H, W):
+        r = r.permute(0, 2, 3, 1)
+    if tuple(r.shape[1:3]) != (H, W):
+        raise ValueError(f"residual must be [{M}, C, rows, cols] or [{M}, rows, cols, C] for shape {(H, W)}")
+    if r.device != ensemble.device:
+        raise ValueError("residual must be on the ensemble's device")
+    if r.dtype not in (torch.float32, torch.bfloat16):
+        r = r.float()
+    nch = int(r.shape[3])
+    if nch not in (1, 3):
+        raise ValueError("residual must have 1 (depth) or 3 (depth, u, v) channels")
+    lim = None
+    if clip_limits is not None and any(c is not None for c in clip_limits):
+        lim = np.stack([np.full(nch, np.inf, np.float32) if c is None else _host_f32(c, nch, "clip_limits")
+                        for c in clip_limits])
+    if out is None:
+        out = [SWEState(*(torch.empty((H, W), dtype=torch.float32, device=ensemble.device) for _ in range(3)))
+               for _ in range(M)]
+    out = [_check_state(st, d) for st, d in zip(out, doms)]
+    with torch.cuda.device(ensemble.device):
+        rc = ensemble._lib.swe_ensemble_apply_correction(
+            ensemble._handle, _ptrs([st.h for st in predicted]), _ptrs([st.hu for st in predicted]),
+            _ptrs([st.hv for st in predicted]), _pitches(predicted), _ptr(r), 1 if r.dtype == torch.bfloat16 else 0,
+            int(r.stride(0)), int(r.stride(1)), int(r.stride(2)), int(r.stride(3)), nch,
+            lim.ctypes.data if lim is not None else None, float(correction_relaxation),
+            _ptrs([st.h for st in out]), _ptrs([st.hu for st in out]), _ptrs([st.hv for st in out]), _pitches(out),
+            _stream(ensemble.device))
+    _lib.check(rc, "ensemble_apply_correction")
+    return out
+
+
 def run_coupled_ensemble(ensemble, initial_states, model, hybrid_inputs: HybridInputs, output_times_s, *,
                          max_substeps_per_interval: int, correction_relaxation: float = 0.05,
                          correction_clip_sigma: float = 5.0, feature_layout: str = "state5",
@@ -419,9 +525,8 @@ def run_coupled_ensemble(ensemble, initial_states, model, hybrid_inputs: HybridI
     corrector = _Corrector(model, dev, overlap)
     with torch.no_grad():
         for k in range(1, T):
-            for m in range(M):
-                network_features(doms[m], cur[m], his[m], times[k - 1], layout=feature_layout, dtype=fdtype,
-                                 out=feats[m], _planes=planes[m])
+            ensemble_network_features(ensemble, cur, his, times[k - 1], layout=feature_layout, out=feats,
+                                      doms=doms, planes=planes)
             x = feats.permute(0, 3, 1, 2)
             started = corrector.start(x)
             res = ensemble.advance_to_(cur, times[k - 1], times[k], int(max_substeps_per_interval))
@@ -434,10 +539,9 @@ def run_coupled_ensemble(ensemble, initial_states, model, hybrid_inputs: HybridI
                 if not t >= times[k] - 1.0e-6:
                     _nan_fill(cur[m])
             residual = corrector.finish(x, started)
+            ensemble_apply_correction(ensemble, cur, residual, correction_relaxation=correction_relaxation,
+                                      clip_limits=lims, out=cur, doms=doms)
             for m in range(M):
-                apply_residual_correction(doms[m], cur[m], residual[m:m + 1],
-                                          correction_relaxation=correction_relaxation, clip_limits=lims[m],
-                                          out=cur[m])
                 if keep_states:
                     for q in range(3):
                         traj[m][q][k].copy_(cur[m][q])

@@ -311,7 +311,9 @@ int swe_ensemble_advance(swe_ensemble_t e, float *const *h, float *const *hu, fl
  * (hybrid/coupled_forecast.py:123-161) for a batch of members, as 50-step
  * graphs until all members are done.  dt_logs: NULL, or per member a device
  * float64 [max_steps] log of its dts (as swe_advance_to).  SWE_ERR_MAX_STEPS
- * when a member did not reach the target (its result says which). */
+ * when a member did not reach the target (its result says which).
+ * Both advances return with their results final and the members' new states
+ * queued on `stream` (stream-ordered, like every call that takes a stream). */
 int swe_ensemble_advance_to(swe_ensemble_t e, float *const *h, float *const *hu, float *const *hv,
                             const int64_t *pitch, const double *start_s, double target_s, int32_t max_steps,
                             double *const *dt_logs, swe_run_result *results, void *stream);
@@ -321,6 +323,27 @@ int swe_ensemble_member(swe_ensemble_t e, int32_t m, swe_domain_t *out);
 int swe_ensemble_set_timing(swe_ensemble_t e, int32_t enable);
 int swe_ensemble_last_step_time(swe_ensemble_t e, double *ms, int64_t *steps);
 int64_t swe_ensemble_last_launch_count(swe_ensemble_t e);
+
+/* The coupling calls of every member in one call (the hybrid ensemble rollout's
+ * per-interval features and corrections; each is swe_network_features /
+ * swe_apply_correction on member m, queued in member order on `stream`).
+ * Arrays hold one entry per member.  Features: mean/stddev are n_members rows
+ * of 5 floats (the first 3 used by REFERENCE6); terrain/roughness NULL or
+ * per-member device pointers (entries may be NULL); member m's features start
+ * at out + m * out_member_stride elements.  Correction: member m's residual
+ * starts at residual + m * res_stride_member elements; clip_limits NULL or
+ * n_members rows of res_channels floats. */
+int swe_ensemble_network_features(swe_ensemble_t e, float *const *h, float *const *hu, float *const *hv,
+                                  const int64_t *pitch, int32_t layout, const float *mean, const float *stddev,
+                                  const float *rain_features, const float *const *terrain,
+                                  const float *const *roughness, void *out, int64_t out_member_stride,
+                                  int32_t out_bf16, void *stream);
+int swe_ensemble_apply_correction(swe_ensemble_t e, float *const *h, float *const *hu, float *const *hv,
+                                  const int64_t *pitch, const void *residual, int32_t residual_bf16,
+                                  int64_t res_stride_member, int64_t res_stride_row, int64_t res_stride_col,
+                                  int64_t res_stride_channel, int32_t res_channels, const float *clip_limits,
+                                  double relaxation, float *const *h_out, float *const *hu_out,
+                                  float *const *hv_out, const int64_t *out_pitch, void *stream);
 
 /* ---- Row strips: one domain split across GPUs ----------------------------
  * (No counterpart in the reference, which runs one domain on one device; the

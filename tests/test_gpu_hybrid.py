@@ -294,3 +294,42 @@ def test_overlapped_corrector_gives_the_same_rollout(cuda_device):
     assert a.physics_steps_used == b.physics_steps_used
     for x, y in zip(a.states, b.states):
         assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("layout,dtype", [("reference6", torch.float32), ("state5", torch.bfloat16)])
+def test_ensemble_coupling_calls_equal_per_member_calls(cuda_device, layout, dtype):
+    """One batched features call and one batched correction call over an
+    ensemble give every member exactly what the per-member calls give."""
+    from hybrid_flood_b200.ensemble import B200Ensemble
+    from hybrid_flood_b200.hybrid import (LAYOUTS, apply_residual_correction, ensemble_apply_correction,
+                                          ensemble_domains, ensemble_network_features, network_features)
+    from hybrid_flood_b200.workloads import urban
+
+    members, states, his = [], [], []
+    for m in range(3):
+        w = urban(40, 56, seed=40 + m, rain_scale=1.0 + 0.5 * m, duration_s=3600.0)
+        members.append(dict(bed=w.bed, manning_n=w.manning_n, domain_mask=w.domain_mask, **w.solver_kwargs()))
+        rng = np.random.default_rng(70 + m)
+        h = np.where(w.domain_mask, rng.uniform(0.0, 0.2, w.shape), 0.0).astype(np.float32)
+        hu = np.where(h > 1e-3, rng.normal(0, 0.02, w.shape), 0.0).astype(np.float32)
+        states.append(_dev((h, hu, np.zeros_like(h) + 0.001), cuda_device))
+        his.append(_inputs(w, np.random.default_rng(80 + m), layout, nres=3))
+    ens = B200Ensemble(members, arithmetic="exact")
+    doms = ensemble_domains(ens)
+    C = LAYOUTS[layout][1]
+    batch = torch.full((3, 40, 56, C), 7.0, dtype=dtype, device=cuda_device)
+    ensemble_network_features(ens, states, his, 1234.5, layout=layout, out=batch)
+    for m in range(3):
+        one = network_features(doms[m], states[m], his[m], 1234.5, layout=layout, dtype=dtype)
+        assert torch.equal(batch[m], one[0])
+    # residual as a corrector returns it: NCHW logical, channels-last memory, bfloat16
+    g = torch.Generator(device="cpu").manual_seed(9)
+    res = (0.05 * torch.randn((3, 3, 40, 56), generator=g)).to(cuda_device, torch.bfloat16)
+    res = res.contiguous(memory_format=torch.channels_last)
+    lims = [np.array([0.02, 0.03, 0.04], np.float32), None, np.array([0.5, 0.5, 0.5], np.float32)]
+    got = ensemble_apply_correction(ens, states, res, correction_relaxation=0.7, clip_limits=lims)
+    for m in range(3):
+        want = apply_residual_correction(doms[m], states[m], res[m:m + 1], correction_relaxation=0.7,
+                                         clip_limits=lims[m])
+        for a, b in zip(got[m], want):
+            assert torch.equal(a, b)
