@@ -333,3 +333,52 @@ def test_ensemble_coupling_calls_equal_per_member_calls(cuda_device, layout, dty
                                          clip_limits=lims[m])
         for a, b in zip(got[m], want):
             assert torch.equal(a, b)
+
+
+def test_coupling_matches_the_reference_coupling_code(cuda_device):
+    """The CUDA coupling against ``tests/golden/coupling_ref6.npz``: outputs of the
+    reference's own ``coupled_forecast.py`` run with a NumPy stand-in for jax
+    (make_coupling_golden.py).  Features bit for bit; correction within 4 ulp
+    (float64 volume sums here, float32 there); the forecast with the same
+    linear corrector as a 1x1 convolution: the same step count, 1e-5 relative L2."""
+    from conftest import golden
+    from hybrid_flood_b200.boundary import BoundaryConfig
+    from hybrid_flood_b200.hybrid import (HybridInputs, apply_residual_correction, network_features,
+                                          run_coupled_forecast)
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver
+
+    torch.backends.cudnn.allow_tf32 = False
+    z = golden("coupling_ref6")
+    bnd = BoundaryConfig(tuple(int(b) for b in z["boundary"]))
+    solver = B200ShallowWaterSolver(z["bed"], z["manning_n"], z["domain_mask"], resolution_m=float(z["dx"]),
+                                    rainfall_times_s=z["rain_times"], rainfall_rates_m_s=z["rain_rates"],
+                                    default_rainfall_m_s=float(z["default_rain"]), boundaries=bnd,
+                                    arithmetic="exact")
+    hi = HybridInputs(z["terrain_std"], z["roughness_std"], z["state_mean"], z["state_std"], float(z["rain_scale"]),
+                      z["residual_std"])
+    st = _dev(tuple(z["state"]), cuda_device)
+    for tag in ("break", "past"):
+        f = network_features(solver, st, hi, float(z[f"features_{tag}_time"]), layout="reference6")
+        np.testing.assert_array_equal(f.cpu().numpy(), z[f"features_{tag}"])
+    lim = z["clip_sigma"] * z["residual_std"]
+    res = torch.tensor(z["residual"], device=cuda_device)
+    got = apply_residual_correction(solver, st, res, correction_relaxation=float(z["relaxation"]), clip_limits=lim)
+    for a, q in zip(got, ("h", "hu", "hv")):
+        assert max_ulp(a.cpu().numpy(), z[f"corrected_{q}"]) <= 4, q
+
+    fs = B200ShallowWaterSolver(z["forecast_bed"], z["forecast_manning_n"], z["forecast_mask"],
+                                resolution_m=float(z["dx"]), rainfall_times_s=[0.0, 1000.0],
+                                rainfall_rates_m_s=[2.0e-5, 2.0e-5], boundaries=bnd, arithmetic="exact")
+    fhi = HybridInputs(z["forecast_terrain_std"], z["forecast_roughness_std"], z["forecast_state_mean"],
+                       z["forecast_state_std"], 25.0, z["forecast_residual_std"])
+    net = torch.nn.Conv2d(6, 3, 1)
+    with torch.no_grad():
+        net.weight.copy_(torch.from_numpy(z["forecast_W"].T.copy())[:, :, None, None])
+        net.bias.copy_(torch.from_numpy(z["forecast_b"]))
+    out = run_coupled_forecast(fs, _dev(tuple(z["forecast_state"]), cuda_device), net.to(cuda_device).eval(), fhi,
+                               z["forecast_times"].astype(np.float64), max_substeps_per_interval=400,
+                               correction_relaxation=0.5, correction_clip_sigma=2.0)
+    assert out.physics_steps_used == int(z["forecast_steps"])
+    for q, name in enumerate(("h", "hu", "hv")):
+        for k in range(len(z["forecast_times"])):
+            assert rel_l2(out.states[q][k].cpu().numpy(), z[f"forecast_{name}"][k]) < 1e-5, (k, name)
