@@ -866,8 +866,8 @@ def run_b200(args, rank: int, world: int):
     stream = torch.cuda.current_stream(dev)
     # Resident state: W untimed warm-up steps, then exactly K timed steps.
     solver.resident_load(state, t_sim)
-    solver.resident_steps(args.warmup)
-    # The graphs of the K timed steps are captured now, outside the timed region.
+    # The graphs of the warm-up and timed steps are captured now, outside the timed region.
+    solver.resident_prepare(args.warmup)
     solver.resident_prepare(args.steps)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clocks:
@@ -875,9 +875,11 @@ def run_b200(args, rank: int, world: int):
             dist.barrier()
         torch.cuda.synchronize(dev)
         clocks.mark_start()
-        # A ~0.1 ms sleep kernel ahead of the start event keeps the stream busy
-        # while the host enqueues the steps, so the region holds no host latency.
+        # A ~0.1 ms sleep kernel and the W warm-up steps run ahead of the start
+        # event: the host enqueues the timed steps while they run (the region
+        # holds no host latency), and the GPU enters the region under load.
         torch.cuda._sleep(200_000)
+        solver.resident_steps(args.warmup)
         start.record(stream)
         solver.resident_steps(args.steps)
         end.record(stream)

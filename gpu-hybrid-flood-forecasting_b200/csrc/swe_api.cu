@@ -1593,7 +1593,10 @@ int swe_resident_prepare(swe_domain_t d, int32_t n_steps) {
     if (!d) return fail(SWE_ERR_INVALID, "null domain");
     if (!d->resident) return fail(SWE_ERR_INVALID, "no resident state: call swe_resident_load first");
     if (n_steps < 0) return fail(SWE_ERR_INVALID, "n_steps must be >= 0");
-    return enqueue_run_steps(d, d->resident_steps, n_steps, nullptr, false);
+    // Both starting buffers: the steps may follow an odd number of other steps.
+    const int rc = enqueue_run_steps(d, d->resident_steps, n_steps, nullptr, false);
+    if (rc) return rc;
+    return enqueue_run_steps(d, d->resident_steps + 1, n_steps, nullptr, false);
 }
 
 int swe_resident_store(swe_domain_t d, float* h, float* hu, float* hv, int64_t pitch, swe_run_result* result,

@@ -372,7 +372,8 @@ class B200ShallowWaterSolver:
         _lib.check(rc, "resident_steps")
 
     def resident_prepare(self, n_steps: int) -> None:
-        """Capture the step graphs the next ``n_steps`` resident steps use, without running them."""
+        """Capture the step graphs that a call of ``n_steps`` resident steps uses, from either
+        ping-pong buffer, without running them."""
         with torch.cuda.device(self.device):
             rc = self._lib.swe_resident_prepare(self._handle, int(n_steps))
         _lib.check(rc, "resident_prepare")

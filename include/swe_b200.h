@@ -149,8 +149,9 @@ int swe_advance(swe_domain_t d, float *h, float *hu, float *hv, int64_t pitch, i
  *                       waiting (as CUDA graphs of up to 32 steps, captured on
  *                       first use);
  *   swe_resident_prepare captures, without running anything, the graphs that
- *                       the next n_steps steps will use, so that the later
- *                       swe_resident_steps only launches;
+ *                       a call of n_steps steps uses, from either ping-pong
+ *                       buffer (it may follow other steps), so that the
+ *                       later swe_resident_steps only launches;
  *   swe_resident_store  copies the current state out and reports the clock,
  *                       the steps taken since the load and the FP64 ledger
  *                       (it synchronises the stream).
