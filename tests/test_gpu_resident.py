@@ -121,3 +121,29 @@ def test_run_to_host_equals_run(cuda_device):
         np.testing.assert_array_equal(x.cpu().numpy(), y)
     with pytest.raises(RuntimeError, match="max_steps"):
         s.run_to_host(host, times, max_steps=3)
+
+
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+def test_runs_follow_a_manning_change(cuda_device, arith):
+    """After set_manning on a domain that has already run (its step graphs
+    captured), a run equals one on a domain created with the new n (ragged
+    last strip, masked cells)."""
+    from hybrid_flood_b200.adjoint import set_manning
+    from hybrid_flood_b200.solver import B200ShallowWaterSolver
+    from hybrid_flood_b200.workloads import street_depth, urban
+
+    w = urban(96, 200, seed=9)
+    mask = w.domain_mask.copy()
+    mask[40:47, 60:70] = False
+    kw = w.solver_kwargs()
+    s = B200ShallowWaterSolver(w.bed, w.manning_n, mask, **kw, arithmetic=arith)
+    init = s.initial_state(depth_m=street_depth(w))
+    s.advance(init, 20, 0.0)
+    n2 = (w.manning_n * np.where(np.arange(w.shape[1]) % 64 < 2, 3.0, 0.5)[None, :]).astype(np.float32)
+    set_manning(s, torch.tensor(n2, device=cuda_device))
+    fresh = B200ShallowWaterSolver(w.bed, n2, mask, **kw, arithmetic=arith)
+    a, ta, na, la = s.advance(init, 60, 0.0)
+    b, tb, nb, lb = fresh.advance(init, 60, 0.0)
+    assert (ta, na) == (tb, nb)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
