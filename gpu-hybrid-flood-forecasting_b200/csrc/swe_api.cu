@@ -106,6 +106,8 @@ struct swe_domain {
     int rparts_cap = 0;
     float* ping[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int64_t ppitch = 0;
+    float* edge_buf[2] = {nullptr, nullptr};  // strip-boundary columns per ping buffer (dd.edge)
+    float* edge_stat = nullptr;               // their bed and n^2 (dd.edge_static)
     float* times_dev = nullptr;
     int times_cap = 0;
     cudaEvent_t poll_ev[2] = {nullptr, nullptr};
@@ -330,6 +332,27 @@ int ensure_parts(swe_domain* d, int blocks) {
     return SWE_OK;
 }
 
+// The bed and n^2 of the strip-boundary columns (when the domain keeps them;
+// after creation and after every change of n^2).
+int fill_edge_statics(swe_domain* d, cudaStream_t st) {
+    if (!d->edge_stat) return SWE_OK;
+    const int nb = (d->dd.cols + kEdgeStrip - 1) / kEdgeStrip + 1;
+    edge_fill_kernel<<<dim3((unsigned)((d->dd.rows + 127) / 128), (unsigned)nb), 128, 0, st>>>(
+        d->dd, StateView{nullptr, nullptr, nullptr, 0}, nullptr, d->edge_stat);
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
+// The strip-boundary columns of the state in ping buffer 0 (a run's start).
+int fill_edges(swe_domain* d, cudaStream_t st) {
+    if (!d->edge_buf[0]) return SWE_OK;
+    const int nb = (d->dd.cols + kEdgeStrip - 1) / kEdgeStrip + 1;
+    edge_fill_kernel<<<dim3((unsigned)((d->dd.rows + 127) / 128), (unsigned)nb), 128, 0, st>>>(
+        d->dd, StateView{d->ping[0][0], d->ping[0][1], d->ping[0][2], d->ppitch}, d->edge_buf[0], nullptr);
+    SWE_CK(cudaGetLastError());
+    return SWE_OK;
+}
+
 int ensure_ping(swe_domain* d) {
     if (d->ping[0][0]) return SWE_OK;
     d->ppitch = round_up(d->dd.cols, 128);
@@ -339,6 +362,29 @@ int ensure_ping(swe_domain* d) {
             SWE_CK(cudaMalloc(&d->ping[b][f], plane));
             SWE_CK(cudaMemset(d->ping[b][f], 0, plane));
         }
+    // The strip-boundary columns that the plain run-mode step keeps for the
+    // next step (DomainDev::edge), allocated with the state buffers, before any
+    // step graph is captured.  Not for row strips of a decomposed domain, whose
+    // halo rows are exchanged outside the step.
+    if (d->strip_total_rows < 0) {
+        DomainDev& dd = d->dd;
+        const int nb = (dd.cols + kEdgeStrip - 1) / kEdgeStrip + 1;
+        dd.edge_rows = round_up(dd.rows, 32);
+        const size_t n6 = sizeof(float) * (size_t)nb * 6 * (size_t)dd.edge_rows;
+        const size_t n4 = sizeof(float) * (size_t)nb * 4 * (size_t)dd.edge_rows;
+        for (int b = 0; b < 2; ++b) {
+            SWE_CK(cudaMalloc(&d->edge_buf[b], n6));
+            SWE_CK(cudaMemset(d->edge_buf[b], 0, n6));
+        }
+        SWE_CK(cudaMalloc(&d->edge_stat, n4));
+        SWE_CK(cudaMemset(d->edge_stat, 0, n4));
+        dd.edge[0] = d->edge_buf[0];
+        dd.edge[1] = d->edge_buf[1];
+        dd.edge_static = d->edge_stat;
+        const int rc = fill_edge_statics(d, nullptr);
+        if (rc) return rc;
+        SWE_CK(cudaDeviceSynchronize());
+    }
     return SWE_OK;
 }
 
@@ -373,6 +419,8 @@ int begin_run(swe_domain* d, StateView init, const float* times_host, int n_time
         rc = copy_plane(d->ping[0][f], d->ppitch, src, init.pitch, rows, cols, st);
         if (rc) return rc;
     }
+    rc = fill_edges(d, st);
+    if (rc) return rc;
     if (n_times > d->times_cap) {
         if (d->times_dev) cudaFree(d->times_dev);
         d->times_dev = nullptr;
@@ -595,6 +643,9 @@ void free_domain(swe_domain* d) {
     cudaFree(d->rparts);
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 3; ++f) cudaFree(d->ping[b][f]);
+    cudaFree(d->edge_buf[0]);
+    cudaFree(d->edge_buf[1]);
+    cudaFree(d->edge_stat);
     cudaFree(d->times_dev);
     for (int q = 0; q < 3; ++q) cudaFree(d->lupd[q]);
     cudaFree(d->times64_dev);
@@ -1228,6 +1279,8 @@ int swe_domain_set_manning(swe_domain_t d, const float* manning_n, int32_t on_ho
     const int64_t n = (int64_t)rows * d->dd.spitch;
     repack_manning_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(src, rows, cols, d->dd.spitch, d->nm);
     SWE_CK(cudaGetLastError());
+    const int erc = fill_edge_statics(d, st);
+    if (erc) return erc;
     if (staged) {
         SWE_CK(cudaStreamSynchronize(st));
         cudaFree(staged);

@@ -69,7 +69,30 @@ struct DomainDev {
     // strip of a decomposed domain also holds its neighbours' boundary rows
     // (halo rows) outside that range: read as ordinary neighbours, never updated.
     int upd_lo, upd_hi;
+    // Strip-boundary columns of the state, kept by the plain run-mode step for
+    // the next step's strip edges (null: not kept; the edges are then loaded
+    // from the state).  For boundary b (between the kEdgeStrip-column strips
+    // b-1 and b) edge[p] holds h, hu, hv of its left cell (column
+    // kEdgeStrip*b - 1) and of its right cell (column kEdgeStrip*b) of the
+    // state in ping-pong buffer p, and edge_static the bed and n^2 of the same
+    // cells: one run of edge_rows floats per boundary, quantity and cell side,
+    // rows contiguous, so that a warp reads 32 rows of an edge in one access.
+    float* edge[2];
+    const float* edge_static;
+    int edge_rows;
 };
+
+constexpr int kEdgeStrip = 64;  // columns of a warp strip of the paired march (32 lanes x 2 cells)
+
+// Index of row r of quantity q of boundary b: q = 0..2 h, hu, hv of the left
+// cell, 3..5 of the right cell (edge); q = 0, 1 bed and n^2 of the left cell,
+// 2, 3 of the right cell (edge_static).
+__host__ __device__ __forceinline__ int64_t edge_index(const DomainDev& d, int b, int q, int r) {
+    return ((int64_t)b * 6 + q) * d.edge_rows + r;
+}
+__host__ __device__ __forceinline__ int64_t edge_static_index(const DomainDev& d, int b, int q, int r) {
+    return ((int64_t)b * 4 + q) * d.edge_rows + r;
+}
 
 struct StateView {
     const float* h;
@@ -145,6 +168,31 @@ struct Control {
 
 // Bytes of the control block the host reads back (everything before the maxima).
 constexpr size_t kControlHead = offsetof(Control, maxk);
+
+// The strip-boundary columns of state `s` into `edge` and, when `stat` is not
+// null, of the bed and n^2 into `stat` (the layouts of DomainDev::edge and
+// edge_static).  Grid: x over the rows, y over the boundaries.  Cells outside
+// the grid (left of boundary 0, right of the last) are left as they are.
+__global__ void edge_fill_kernel(const DomainDev d, const StateView s, float* edge, float* stat) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y;
+    if (r >= d.rows) return;
+    for (int side = 0; side < 2; ++side) {
+        const int x = kEdgeStrip * b - 1 + side;
+        if (x < 0 || x >= d.cols) continue;
+        if (edge) {
+            const int64_t so = (int64_t)r * s.pitch + x;
+            edge[edge_index(d, b, 3 * side + 0, r)] = s.h[so];
+            edge[edge_index(d, b, 3 * side + 1, r)] = s.hu[so];
+            edge[edge_index(d, b, 3 * side + 2, r)] = s.hv[so];
+        }
+        if (stat) {
+            const int64_t zo = (int64_t)r * d.spitch + x;
+            stat[edge_static_index(d, b, 2 * side + 0, r)] = d.bed[zo];
+            stat[edge_static_index(d, b, 2 * side + 1, r)] = d.nm[zo];
+        }
+    }
+}
 
 // A run's control block written from launch parameters: the head as the host
 // built it, the stripe maxima zeroed and up to two target times.  Parameters

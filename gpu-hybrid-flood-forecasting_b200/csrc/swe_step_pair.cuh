@@ -77,10 +77,21 @@ __device__ __forceinline__ float2 lfma(float2 a, float2 b, float2 c) { return __
 // LAST_CONSUME: the last row also consumes (zero-byte copies past the chunk,
 // values unused), which keeps the row body free of that branch; the plain step
 // measured 0.6 % faster with it, the ensemble kernel spills with it.
-template <class M, bool RUN, bool MASKED, bool LAST_CONSUME, class PlanFn>
+//
+// EDGES (the plain run-mode step): with epar >= 0, the domain keeps its
+// strip-boundary columns (DomainDev::edge) and `in` is ping-pong buffer epar.
+// The strip edges are then read from edge[epar] where the neighbouring cells
+// lie inside the grid (one coalesced access per quantity for 32 rows, where
+// the state would need one cache line per row), and lanes 0 and 31 write the
+// strip's first and last columns of `out` into edge[epar ^ 1] for the next
+// step.  The 2048^2 step measured 7 % faster with it; the ensemble kernel
+// loads its strip edges from the state.
+static_assert(kEdgeStrip == 2 * kWarp, "a paired-march strip is 2 x 32 columns");
+
+template <class M, bool RUN, bool MASKED, bool LAST_CONSUME, bool EDGES, class PlanFn>
 __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& in,
                                             const StateOut& out, PlanFn&& plan_fn, const Control* ctl,
-                                            int r0, int r1, int x0w, WarpSmem& sm, StepAccum& acc) {
+                                            int r0, int r1, int x0w, WarpSmem& sm, StepAccum& acc, int epar = -1) {
     constexpr int kBatch = kWarp;
     using A = P<M>;
     const Consts& k = d.k;
@@ -114,6 +125,13 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
         if constexpr (A::kExact) return pow2 ? A::mul(a, rdye) : A::div(a, dy2);
         else return A::mul(a, rdye);
     };
+    // This lane's column run of the next step's edges (lanes 0 and 31), or null.
+    float* ep = nullptr;
+    if (EDGES && epar >= 0) {
+        const int eb = x0w / kEdgeStrip;
+        if (lane == 0) ep = d.edge[epar ^ 1] + edge_index(d, eb, 3, 0);
+        else if (lane == kWarp - 1 && valid.y) ep = d.edge[epar ^ 1] + edge_index(d, eb + 1, 0, 0);
+    }
     const int nq = r1 - r0 + 2;  // rows r0-1 .. r1 pass through the ring
     const bool edge_strip = x0w + kWarp * 2 > d.cols;
     const int csize = valid.y ? 8 : (valid.x ? 4 : 0);
@@ -340,6 +358,12 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
             out.hu[so] = o.hu.x;
             out.hv[so] = o.hv.x;
         }
+        if (EDGES && ep != nullptr) {
+            const bool first = lane == 0;
+            ep[r] = first ? o.h.x : o.h.y;
+            ep[r + d.edge_rows] = first ? o.hu.x : o.hu.y;
+            ep[r + 2 * d.edge_rows] = first ? o.hv.x : o.hv.y;
+        }
         if (RUN && snap >= 0) {
             const Control* c = ctl;
             const int64_t base = (int64_t)snap * c->out_plane + (int64_t)r * d.cols + c0;
@@ -360,9 +384,26 @@ __device__ __forceinline__ bool march_pair(const DomainDev& d, const StateView& 
         __syncwarp();
         const int rr = min(rb + lane, d.rows - 1);
         Cell L[1], E[1], Q[1];
-        load_cells<1>(d, in, rr, x0w - 1, L);
-        load_cells<1>(d, in, rr, x0w, E);
-        load_cells<1>(d, in, rr, x0w + kWarp * 2, Q);
+        const int b = x0w / kEdgeStrip;
+        const float* ein = EDGES && epar >= 0 ? d.edge[epar] : nullptr;
+        if (EDGES && ein != nullptr && x0w > 0) {
+            L[0] = {__ldg(ein + edge_index(d, b, 0, rr)), __ldg(ein + edge_index(d, b, 1, rr)),
+                    __ldg(ein + edge_index(d, b, 2, rr)), __ldg(d.edge_static + edge_static_index(d, b, 0, rr)),
+                    __ldg(d.edge_static + edge_static_index(d, b, 1, rr)), 0.f, 0.f};
+            E[0] = {__ldg(ein + edge_index(d, b, 3, rr)), __ldg(ein + edge_index(d, b, 4, rr)),
+                    __ldg(ein + edge_index(d, b, 5, rr)), __ldg(d.edge_static + edge_static_index(d, b, 2, rr)),
+                    __ldg(d.edge_static + edge_static_index(d, b, 3, rr)), 0.f, 0.f};
+        } else {
+            load_cells<1>(d, in, rr, x0w - 1, L);
+            load_cells<1>(d, in, rr, x0w, E);
+        }
+        if (EDGES && ein != nullptr && x0w + kEdgeStrip < d.cols) {
+            Q[0] = {__ldg(ein + edge_index(d, b + 1, 3, rr)), __ldg(ein + edge_index(d, b + 1, 4, rr)),
+                    __ldg(ein + edge_index(d, b + 1, 5, rr)), __ldg(d.edge_static + edge_static_index(d, b + 1, 2, rr)),
+                    __ldg(d.edge_static + edge_static_index(d, b + 1, 3, rr)), 0.f, 0.f};
+        } else {
+            load_cells<1>(d, in, rr, x0w + kWarp * 2, Q);
+        }
         CellT<float> l{L[0].h, L[0].hu, L[0].hv, L[0].z, L[0].nm, 0.f, 0.f};
         CellT<float> e{E[0].h, E[0].hu, E[0].hv, E[0].z, E[0].nm, 0.f, 0.f};
         CellT<float> q{Q[0].h, Q[0].hu, Q[0].hv, Q[0].z, Q[0].nm, 0.f, 0.f};
@@ -477,8 +518,9 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
             return MarchPlan{pl.s, pl.snap, pl.dt, pl.go};
         };
         const bool went = r0 < d.upd_hi
-                              ? march_pair<M, true, MASKED, true>(d, p.in, p.out, plan_fn, p.ctl, r0, r1, strip * kWarp * 2,
-                                                            s_warp[wib], acc)
+                              ? march_pair<M, true, MASKED, true, true>(d, p.in, p.out, plan_fn, p.ctl, r0, r1,
+                                                                  strip * kWarp * 2, s_warp[wib], acc,
+                                                                  d.edge[0] ? p.par : -1)
                               : plan_fn().go != 0;
         if (!went) {  // uniform over the grid: the run has ended
             cp_async_wait<0>();
@@ -496,7 +538,7 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
         warp_end_step(p.ctl, &p.slots[gw], s_warp[wib].old, p.par, in.pos.steps, gw % kMaxStripes, a);
     } else {
         if (r0 < d.upd_hi)
-            march_pair<M, false, MASKED, true>(d, p.in, p.out, [&]() { return MarchPlan{p.s, -1, 0.0, 1}; }, nullptr, r0,
+            march_pair<M, false, MASKED, true, false>(d, p.in, p.out, [&]() { return MarchPlan{p.s, -1, 0.0, 1}; }, nullptr, r0,
                                          r1, strip * kWarp * 2, s_warp[wib], acc);
     }
 }
@@ -546,7 +588,7 @@ __device__ __forceinline__ void ensemble_item(const MemberDev& md, int slot, int
     const StateOut out{md.buf[par ^ 1][0], md.buf[par ^ 1][1], md.buf[par ^ 1][2], md.pitch};
     StepAccum acc;
     acc.zero();
-    const bool went = r0 < md.d.rows ? march_pair<M, true, MASKED, false>(md.d, in, out, plan_fn, md.ctl, r0, r1,
+    const bool went = r0 < md.d.rows ? march_pair<M, true, MASKED, false, false>(md.d, in, out, plan_fn, md.ctl, r0, r1,
                                                                    strip * kWarp * 2, sm, acc)
                                      : plan_fn().go != 0;
     if (!went) {
