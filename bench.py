@@ -57,7 +57,7 @@ BYTES_PER_CELL = 32  # h, hu, hv, bed, n^2 read (20 B) + h, hu, hv written (12 B
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fast-arithmetic
 # step_kernel_pair launch on the default 2048x2048 workload, per cell-update, from an
 # ncu capture of that launch: reported as roofline.traffic for that configuration only.
-NCU_TRAFFIC_PER_CELL = (107.584768e6 + 14.789632e6) / 4194304
+NCU_TRAFFIC_PER_CELL = (92.77184e6 + 17.041664e6) / 4194304
 REFERENCE_MAX_STEPS = 200  # whole-grid steps the CPU reference arm times at most
 
 
