@@ -84,8 +84,9 @@ __device__ __forceinline__ float2 lfma(float2 a, float2 b, float2 c) { return __
 // lie inside the grid (one coalesced access per quantity for 32 rows, where
 // the state would need one cache line per row), and lanes 0 and 31 write the
 // strip's first and last columns of `out` into edge[epar ^ 1] for the next
-// step.  The 2048^2 step measured 7 % faster with it; the ensemble kernel
-// loads its strip edges from the state.
+// step.  The 2048^2 step measured 7 % faster with it in fast arithmetic; in
+// exact arithmetic (more registers) it spilled and measured 1.5 % slower, and
+// the ensemble kernel loads its strip edges from the state too.
 static_assert(kEdgeStrip == 2 * kWarp, "a paired-march strip is 2 x 32 columns");
 
 template <class M, bool RUN, bool MASKED, bool LAST_CONSUME, bool EDGES, class PlanFn>
@@ -518,7 +519,7 @@ __global__ void __launch_bounds__(THREADS, SWE_PAIR_MINBLOCKS) step_kernel_pair(
             return MarchPlan{pl.s, pl.snap, pl.dt, pl.go};
         };
         const bool went = r0 < d.upd_hi
-                              ? march_pair<M, true, MASKED, true, true>(d, p.in, p.out, plan_fn, p.ctl, r0, r1,
+                              ? march_pair<M, true, MASKED, true, !P<M>::kExact>(d, p.in, p.out, plan_fn, p.ctl, r0, r1,
                                                                   strip * kWarp * 2, s_warp[wib], acc,
                                                                   d.edge[0] ? p.par : -1)
                               : plan_fn().go != 0;
