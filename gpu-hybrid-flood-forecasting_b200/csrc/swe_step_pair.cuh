@@ -84,9 +84,10 @@ __device__ __forceinline__ float2 lfma(float2 a, float2 b, float2 c) { return __
 // lie inside the grid (one coalesced access per quantity for 32 rows, where
 // the state would need one cache line per row), and lanes 0 and 31 write the
 // strip's first and last columns of `out` into edge[epar ^ 1] for the next
-// step.  The 2048^2 step measured 7 % faster with it in fast arithmetic; in
-// exact arithmetic (more registers) it spilled and measured 1.5 % slower, and
-// the ensemble kernel loads its strip edges from the state too.
+// step.  In fast arithmetic the 2048^2 step measured 7 % faster with it and
+// the ensemble of 16 x 1024^2 members (114-row marches) 6 % (the 64-member mix,
+// 256-row marches, the same); in exact arithmetic (more registers) it spilled
+// and measured 1.5 % slower, so exact marches load their edges from the state.
 static_assert(kEdgeStrip == 2 * kWarp, "a paired-march strip is 2 x 32 columns");
 
 template <class M, bool RUN, bool MASKED, bool LAST_CONSUME, bool EDGES, class PlanFn>
@@ -589,8 +590,9 @@ __device__ __forceinline__ void ensemble_item(const MemberDev& md, int slot, int
     const StateOut out{md.buf[par ^ 1][0], md.buf[par ^ 1][1], md.buf[par ^ 1][2], md.pitch};
     StepAccum acc;
     acc.zero();
-    const bool went = r0 < md.d.rows ? march_pair<M, true, MASKED, false, false>(md.d, in, out, plan_fn, md.ctl, r0, r1,
-                                                                   strip * kWarp * 2, sm, acc)
+    const bool went = r0 < md.d.rows ? march_pair<M, true, MASKED, false, !P<M>::kExact>(md.d, in, out, plan_fn, md.ctl,
+                                                                   r0, r1, strip * kWarp * 2, sm, acc,
+                                                                   md.d.edge[0] ? par : -1)
                                      : plan_fn().go != 0;
     if (!went) {
         cp_async_wait<0>();
